@@ -1,0 +1,406 @@
+"""Throughput of the B200 k-mer association test.
+
+Workload (default): n=1,000 samples (8 subpopulations, 5% without phenotype),
+m=200,000,000 k-mers packed 1 bit/sample (16 uint64 words = 128 B per k-mer,
+25.6 GB resident in HBM), U = intercept + 16 PCs, one phenotype with 50 causal
+k-mers, CORR_THRESHOLD=0 (every non-constant k-mer is tested).  Seeded
+synthetic data, generated on the device.
+
+A step = one pass of the association test over the whole batch: pre-filter,
+U^T x and x.y' contraction, chi-square and p, hit compaction, count.
+``value`` times the split-precision tensor-core kernel with the batch resident
+in HBM; ``e2e`` times kg_run_host from pinned host memory (host-to-device
+copies inside the timed region); ``fp64_form`` is the plain FP64 CUDA-core
+kernel on the same batch.  The batch (25.6 GB) is far larger than L2 (126 MB),
+so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(n=1000, m=200_000_000, S=8, r=16, n_causal=50, missing=0.05, seed=44)
+METRIC = "k-mer tests/s (split-precision tcgen05 kernel, n=1000, r=16+1, batch resident in HBM)"
+
+
+def rank_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per k-mer of the split kernel from the committed ncu summary (or None)."""
+    p = os.path.join(ROOT, "profiles", "tc_kernel_n1000_r16.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_kmer:"):
+            return float(line.split(":")[1])
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        try:
+            self.out = tempfile.NamedTemporaryFile("w+", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.dev)], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc or not self.out:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.out.flush()
+        rows = [l.split(", ") for l in open(self.out.name).read().strip().splitlines() if l.count(",") >= 8]
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        sm = [float(r[1]) for r in rows]
+        mx = max(float(r[2]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
+        load = [s for s, r in zip(sm, rows) if float(r[3]) > 200.0] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ------------------------------------------------------------ CPU baseline
+
+def reference_binary():
+    exe = os.path.join(ROOT, "oracle", "_ref", "kgwas")
+    return exe if os.access(exe, os.X_OK) else None
+
+
+def cpu_reference_run(n, m_sample, r, seed, threads, workdir):
+    """Run the reference kgwas (COLS mode) on an m_sample-k-mer batch; returns (tests, seconds)."""
+    from supergwas_b200 import synth
+    from oracle import oracle as O
+    ds = synth.simulate(n=n, m=m_sample, S=WORKLOAD["S"], r=r, n_causal=min(50, m_sample),
+                        missing=WORKLOAD["missing"], seed=seed, structure_kmers=min(50_000, m_sample))
+    paths = synth.write_dataset(workdir, ds)
+    out = os.path.join(workdir, "out", "batch_000.tsv")
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    env = {"CORR_THRESHOLD": "0", "LOAD_THREADS": threads, "BLAS_THREADS": threads, "EMIT_THREADS": threads}
+    t0 = time.perf_counter()
+    res = O.run_reference([paths["samples"], paths["pheno"], paths["batch"], paths["ubin"], out, "6"], env)
+    dt = time.perf_counter() - t0
+    if res.returncode != 0:
+        raise RuntimeError(res.stderr[-500:])
+    tested = int(open(out + ".count").read().split("\t")[1])
+    return tested, dt, paths
+
+
+def cpu_port_run(n, m_sample, r, seed):
+    """The oracle (single-thread C port) on an m_sample-k-mer batch."""
+    from supergwas_b200 import synth
+    from oracle import oracle as O
+    ds = synth.simulate(n=n, m=m_sample, S=WORKLOAD["S"], r=r, n_causal=min(50, m_sample),
+                        missing=WORKLOAD["missing"], seed=seed, structure_kmers=min(50_000, m_sample))
+    X = ds.packed_overlap()
+    t0 = time.perf_counter()
+    st = O.cols_stats(X, ds.n, ds.U, ds.y, 0.0)
+    return st["n_tested"], time.perf_counter() - t0
+
+
+def cpu_baseline(n, r, seed, sample_kmers):
+    threads = os.cpu_count() or 1
+    if reference_binary():
+        with tempfile.TemporaryDirectory() as d:
+            tested, dt, _ = cpu_reference_run(n, sample_kmers, r, seed, threads, d)
+        return {"value": tested / dt, "unit": "k-mer tests/s", "cores": threads, "kind": "reference",
+                "sample": f"reference kgwas --mode cols (shipped binary), n={n}, r={r}+1, "
+                          f"{sample_kmers} k-mers, CORR_THRESHOLD=0, wall clock incl. its file load"}
+    m = max(1000, sample_kmers // 20)
+    tested, dt = cpu_port_run(n, m, r, seed)
+    return {"value": tested / dt, "unit": "k-mer tests/s", "cores": 1, "kind": "port",
+            "sample": f"FP64 C oracle, n={n}, r={r}+1, {m} k-mers, CORR_THRESHOLD=0"}
+
+
+def run_reference_arm(args):
+    """The reference's own CPU implementation on this box's host cores: one
+    batch of ``--ref-kmers`` k-mers of the bench workload, run W + K times."""
+    rank, world, _ = rank_env()
+    if rank != 0:
+        return
+    W = WORKLOAD
+    threads = os.cpu_count() or 1
+    m_sample = args.ref_kmers
+    vals = []
+    kind = "reference" if reference_binary() else "port"
+    with tempfile.TemporaryDirectory() as d:
+        if kind == "reference":
+            from oracle import oracle as O
+            tested, dt, paths = cpu_reference_run(W["n"], m_sample, W["r"], W["seed"], threads, d)
+            env = {"CORR_THRESHOLD": "0", "LOAD_THREADS": threads, "BLAS_THREADS": threads,
+                   "EMIT_THREADS": threads}
+            out = os.path.join(d, "out", "batch_000.tsv")
+            for i in range(args.warmup + args.steps):
+                t0 = time.perf_counter()
+                res = O.run_reference([paths["samples"], paths["pheno"], paths["batch"], paths["ubin"], out,
+                                       "6"], env)
+                dt = time.perf_counter() - t0
+                if res.returncode != 0:
+                    raise RuntimeError(res.stderr[-500:])
+                if i >= args.warmup:
+                    vals.append((int(open(out + ".count").read().split("\t")[1]), dt))
+        else:
+            for i in range(args.warmup + args.steps):
+                tested, dt = cpu_port_run(W["n"], max(1000, m_sample // 20), W["r"], W["seed"])
+                if i >= args.warmup:
+                    vals.append((tested, dt))
+    tests = sum(t for t, _ in vals)
+    secs = sum(s for _, s in vals)
+    v = tests / secs
+    ms = m_sample if kind == "reference" else max(1000, m_sample // 20)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "k-mer tests/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / len(vals),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (reference COLS mode)" if kind == "reference" else "f64",
+            "data": "synthetic",
+            "config": {"workload": f"n={W['n']} (5% unphenotyped), r={W['r']}+1, 1 phenotype, "
+                                   f"CORR_THRESHOLD=0; each step one {ms}-k-mer batch of that workload",
+                       "parallelism": "host cores"},
+            "cpu_baseline": {"value": v, "unit": "k-mer tests/s", "cores": threads if kind == "reference" else 1,
+                             "kind": kind,
+                             "sample": (f"shipped reference kgwas --mode cols on {ms} k-mers per step, wall "
+                                        "clock of the process (file load included)") if kind == "reference"
+                             else f"FP64 C oracle on {ms} k-mers per step"},
+            "e2e": {"value": v, "unit": "k-mer tests/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------- GPU arm
+
+def accuracy_report(X_dev, m_sub, wpk, U, y, keep, n_all):
+    """Split form vs the FP64 oracle on the first m_sub k-mers: chi2 rel / -log10 p abs errors."""
+    from oracle import oracle as O
+    from supergwas_b200 import api, synth
+    Xh = X_dev[:m_sub].cpu().numpy().view(np.uint64)
+    Xo = synth.select_samples(Xh, n_all, keep)
+    o = O.cols_stats(Xo, len(keep), U, y, 0.0)
+    with api.Kgwas(precision="split", corr_threshold=0.0, log10_thresh=6.0) as g:
+        g.set_structure(U, y, keep, n_all)
+        res = g.run_host(Xh, stats=True)
+    st = res.stats
+    msk = st["tested"] & o["tested"]
+    T0, T1 = o["chisq"][msk], st["chisq"][msk]
+    rel = np.abs(T1 - T0) / np.maximum(T0, 1e-300)
+    ml = np.abs(st["mlog10p"][msk] - o["mlog10p"][msk])
+    return {"kmers_checked": int(m_sub), "tested_identical": bool(np.array_equal(st["tested"], o["tested"])),
+            "chisq_rel_max": float(rel.max()), "chisq_rel_p99": float(np.percentile(rel, 99)),
+            "chisq_rel_max_T_ge_1e-3": float(rel[T0 >= 1e-3].max()),
+            "mlog10p_abs_max": float(ml.max()), "mlog10p_abs_p99": float(np.percentile(ml, 99)),
+            "reference": "FP64 C oracle (long-double accumulation)"}
+
+
+def time_device(g, X, m, wpk, steps, warmup, stream):
+    import torch
+    launches = 0
+    for _ in range(warmup):
+        g.launch_device(X.data_ptr(), m, wpk, stream.cuda_stream)
+        g.fetch()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    tested = 0
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+        for i in range(steps):
+            g.launch_device(X.data_ptr(), m, wpk, stream.cuda_stream)
+            launches += g.last_launch_count()
+            ev[i + 1].record(stream)
+    torch.cuda.synchronize()
+    res = g.fetch()
+    tested = res.n_tested
+    per = [ev[i].elapsed_time(ev[i + 1]) for i in range(steps)]
+    return tested, per, launches
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from supergwas_b200 import api, build, synth_gpu
+    rank, world, local = rank_env()
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    build.build_all()
+    W = dict(WORKLOAD)
+    if args.kmers:
+        W["m"] = args.kmers
+    n, m, r = W["n"], W["m"], W["r"]
+    wpk = (n + 63) // 64
+    wpk += wpk & 1
+    t_gen = time.perf_counter()
+    X = synth_gpu.gen_packed(n, m, W["S"], W["seed"] + 1000 * rank)
+    U, y, keep, causal = synth_gpu.structure_and_phenotype(X, n, r, W["n_causal"], W["missing"],
+                                                           W["seed"] + 1000 * rank)
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t_gen
+    stream = torch.cuda.Stream()
+    hbm, bf16, peak_src = measured_peaks()
+
+    g = api.Kgwas(device=local, precision="split", corr_threshold=0.0, log10_thresh=6.0)
+    g.set_structure(U, y, keep, n)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as ck:
+        tested, per, launches = time_device(g, X, m, wpk, args.steps, args.warmup, stream)
+        if world > 1:
+            dist.barrier()
+    clocks = ck.summary()
+    t_split = sum(per) / 1e3
+
+    # plain FP64 form on the same batch
+    f = api.Kgwas(device=local, precision="fp64", corr_threshold=0.0, log10_thresh=6.0)
+    f.set_structure(U, y, keep, n)
+    fsteps = max(1, min(args.steps, 3))
+    ftested, fper, _ = time_device(f, X, m, wpk, fsteps, 1, stream)
+    t_fp64 = sum(fper) / fsteps / 1e3
+
+    # end to end through kg_run_host from pinned host memory
+    m_e2e = min(m, args.e2e_kmers) if args.e2e_kmers else m
+    hbuf = api.lib().kg_host_alloc(m_e2e * wpk * 8)
+    if not hbuf:
+        raise RuntimeError("kg_host_alloc failed")
+    import ctypes
+    hview = (ctypes.c_char * (m_e2e * wpk * 8)).from_address(hbuf)
+    ht = torch.frombuffer(hview, dtype=torch.int64).view(m_e2e, wpk)
+    ht.copy_(X[:m_e2e])
+    torch.cuda.synchronize()
+    e2e_steps = max(1, min(args.steps, 5))
+    g.run_host_ptr(hbuf, m_e2e, wpk)  # warm-up (allocates chunk buffers)
+    t0 = time.perf_counter()
+    e2e_tested = 0
+    for _ in range(e2e_steps):
+        rr = g.run_host_ptr(hbuf, m_e2e, wpk)
+        e2e_tested += rr.n_tested
+    t_e2e = (time.perf_counter() - t0) / e2e_steps
+    d2h = 3 * 8 + rr.hits.shape[0] * 32
+    api.lib().kg_host_free(hbuf)
+
+    # max over ranks of device time; sum of tests
+    if world > 1:
+        tt = torch.tensor([t_split, float(tested)], dtype=torch.float64, device="cuda")
+        mx = tt.clone()
+        dist.all_reduce(mx[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(tt[1:], op=dist.ReduceOp.SUM)
+        t_split_all = float(mx[0])
+        tested_all = float(tt[1])
+    else:
+        t_split_all = t_split
+        tested_all = float(tested)
+
+    if rank == 0:
+        value = tested_all * args.steps / t_split_all
+        t_launch = t_split / args.steps
+        alg_bytes = m * ((n + 7) // 8)          # packed x, 1 bit per sample (algorithmic)
+        achieved = alg_bytes / t_launch / 1e9
+        traffic_pk = profile_traffic()
+        N = 64
+        kpad = ((n + 255) // 256) * 256
+        tops = 2.0 * m * kpad * N / t_launch / 1e12
+        acc = accuracy_report(X, min(m, args.acc_kmers), wpk, U, y, keep, n)
+        cpu = cpu_baseline(n, r, W["seed"], args.cpu_kmers) if not args.no_cpu else None
+        line = {
+            "metric": METRIC, "value": value, "unit": "k-mer tests/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_split_all / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "i8 limbs -> i32 TMEM, f64 epilogue",
+            "data": "synthetic (seeded Balding-Nichols, generated on device)",
+            "config": {"workload": f"n={n} (5% unphenotyped), m={m} k-mers per GPU, r={r}+1, 1 phenotype, "
+                                   f"CORR_THRESHOLD=0", "kmers_per_gpu": m, "bytes_per_kmer": wpk * 8,
+                       "l2": "inputs (%.1f GB) >> L2; no flush needed" % (m * wpk * 8 / 1e9),
+                       "parallelism": f"weak: {world} GPU(s), independent k-mer shards"},
+            "tests_per_step": tested_all,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_source": peak_src,
+                         "traffic": (traffic_pk * m if traffic_pk else None),
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "tensor": {"achieved_tops_int8": tops, "peak_tops_int8": 2 * bf16,
+                                    "frac": tops / (2 * bf16),
+                                    "peak_note": "2x measured bf16 burst (int8 MMA issues at twice the bf16 rate)"}},
+            "fp64_form": {"value": ftested / t_fp64, "unit": "k-mer tests/s", "ms_per_step": 1e3 * t_fp64,
+                          "split_speedup": value / world / (ftested / t_fp64)},
+            "accuracy_vs_fp64_oracle": acc,
+            "e2e": {"value": e2e_tested / e2e_steps / t_e2e * world, "unit": "k-mer tests/s",
+                    "h2d_bytes_per_step": m_e2e * wpk * 8, "d2h_bytes_per_step": d2h,
+                    "kmers_per_step": m_e2e, "api": "kg_run_host (pinned host buffer)"},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+            "gen_seconds": t_gen,
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    f.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--kmers", type=int, default=0, help="k-mers per GPU (default 2e8)")
+    ap.add_argument("--e2e-kmers", type=int, default=0, help="k-mers of the end-to-end leg (default all)")
+    ap.add_argument("--acc-kmers", type=int, default=200_000)
+    ap.add_argument("--cpu-kmers", type=int, default=1_000_000)
+    ap.add_argument("--ref-kmers", type=int, default=250_000)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours" and not os.environ.get("KG_BENCH_ALLOW_SHORT"):
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,153 @@
+/*
+ * kgwas_cuda.h -- C ABI of the B200 k-mer association test.
+ *
+ * The reference exposes no library API: its boundary is the `kgwas` process
+ * (src/kgwas.cpp:67-126), whose COLS mode runs, inside one process,
+ *   build_overlap + load_Ubin      (src/kgwas_utils.hpp:129-157, 285-314)
+ *   Pearson pre-filter             (src/kgwas.cpp:182-218)
+ *   compute_cols_stats             (src/kgwas.cpp:138-166)
+ *   compute_hit + emit selection   (src/kgwas.cpp:44-56, 225-259)
+ *   .count                         (src/kgwas.cpp:291-304)
+ * This header replaces the internal seam between the file readers and that
+ * arithmetic.  The `kgwas` program in this package keeps the reference's
+ * command line, readers and output text and calls these functions; other
+ * hosts (Python via ctypes, a job runner) can call them directly.
+ *
+ * Conventions
+ *   - Every function returns KG_OK (0) or a KG_ERR_* code and never exits
+ *     the process; kg_last_error() describes the last failure of a context.
+ *   - One context per GPU and per host thread.  A context owns its device
+ *     buffers and its CUDA stream.
+ *   - Packed k-mer rows: k-mer-major, `words_per_kmer` uint64 words per
+ *     k-mer (even, so every row starts on a 16-byte boundary); overlap
+ *     sample i is bit (i % 64) of word (i / 64); bits at i >= n are ignored.
+ */
+#ifndef KGWAS_CUDA_H
+#define KGWAS_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KG_OK              0
+#define KG_ERR_INVALID     1  /* bad argument or shape                       */
+#define KG_ERR_CUDA        2  /* CUDA runtime / launch failure              */
+#define KG_ERR_NOMEM       3  /* device or pinned host allocation failed     */
+#define KG_ERR_STATE       4  /* call out of order (e.g. no structure set)   */
+#define KG_ERR_TIMEOUT     5  /* a bounded device-side wait gave up          */
+#define KG_ERR_UNSUPPORTED 6  /* shape outside what the kernel supports      */
+
+/* Arithmetic of the contraction U^T x, x.y'. */
+#define KG_PREC_SPLIT_I8 0  /* tcgen05 kind::i8: x exact in int8, U/y' split
+                               into signed int8 limbs, exact int32 TMEM
+                               accumulation, FP64 epilogue (default)        */
+#define KG_PREC_FP64     1  /* plain FP64 on CUDA cores                      */
+
+typedef struct kg_ctx kg_ctx;
+
+typedef struct kg_opts {
+    int device;             /* CUDA device ordinal                                 */
+    int precision;          /* KG_PREC_*                                           */
+    double corr_threshold;  /* CORR_THRESHOLD, default 0.2 (src/kgwas.cpp:30)      */
+    double log10_thresh;    /* emit rows with p <= 10^-log10_thresh, default 6
+                               (src/kgwas.cpp:28,230)                              */
+    int limbs_u;            /* int8 limbs per U column (0 = default 3, at most 4)   */
+    int limbs_y;            /* int8 limbs for y' (0 = default 5, at most 5)         */
+} kg_opts;
+
+/* One emitted row (src/kgwas.cpp:247-255): k-mer index within the call's
+ * input, effect = xyM/(xxM*yyM), p = erfc(sqrt(T/2)), T the 1-df chi-square. */
+typedef struct kg_hit {
+    uint64_t kmer;
+    double effect;
+    double pval;
+    double chisq;
+} kg_hit;
+
+typedef struct kg_result {
+    uint64_t n_kmers;   /* k-mers in the call                                       */
+    uint64_t n_tested;  /* passed the pre-filter: the .count value (src/kgwas.cpp:301) */
+    uint64_t n_hits;    /* rows with p <= 10^-log10_thresh                          */
+    const kg_hit* hits; /* sorted by k-mer index; owned by the context, valid until
+                           the next kg_run_* / kg_fetch / kg_destroy on it           */
+} kg_result;
+
+/* Optional per-k-mer host outputs, each of length n_kmers (any may be NULL).
+ * Untested k-mers get tested=0, chisq=0, pval=1, effect=0, mlog10p=0. */
+typedef struct kg_stats {
+    uint8_t* tested;
+    double* chisq;
+    double* pval;
+    double* effect;
+    double* mlog10p;    /* -log10 p from a log-domain tail (no underflow)   */
+    double* xxM;
+    double* xyM;
+    double* cor;        /* Pearson correlation of the pre-filter             */
+} kg_stats;
+
+/* Fill `opts` with the reference's defaults (device 0, split precision). */
+void kg_default_opts(kg_opts* opts);
+
+/* Create a context on opts->device.  Replaces the process set-up of
+ * src/kgwas.cpp:527-532 / parse_args :67-126 for the arithmetic part. */
+int kg_create(kg_ctx** out, const kg_opts* opts);
+
+/* Set the structure and phenotype of one test.  U is n x k column-major
+ * FP64 (the U.bin body, src/kgwas_utils.hpp:135-157), y the phenotype of the
+ * n overlap samples in samples-file order (src/kgwas_utils.hpp:291-314).
+ * Computes yyM = ||y||^2 - ||U^T y||^2 (src/kgwas_utils.hpp:151-153); stores
+ * it in *yyM_out when non-NULL. */
+int kg_set_structure(kg_ctx* ctx, const double* U_colmajor, int n, int k,
+                     const double* y, double* yyM_out);
+
+/* As kg_set_structure, for packed rows that hold more samples than the
+ * overlap (e.g. every sample of samples.txt, or one row layout shared by many
+ * phenotypes with different missing samples): overlap sample i is bit
+ * sample_pos[i] of each row, rows hold n_row_samples samples, and bits at
+ * every other position are ignored.  Replaces the overlap gather of
+ * load_matrix_rows (src/kgwas_utils.hpp:236-240). */
+int kg_set_structure_ex(kg_ctx* ctx, const double* U_colmajor, int n, int k,
+                        const double* y, const int32_t* sample_pos, int n_row_samples,
+                        double* yyM_out);
+
+/* Run the test on host-resident packed rows (pageable or pinned).  Host to
+ * device copies are chunked and overlapped with the kernels.  Replaces the
+ * pre-filter, compute_cols_stats, compute_hit and the emit selection
+ * (src/kgwas.cpp:182-259) plus the .count value (:301). */
+int kg_run_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t n_kmers,
+                uint32_t words_per_kmer, kg_result* res, kg_stats* stats);
+
+/* Same on device-resident rows.  Enqueues the kernels on `stream`
+ * (a cudaStream_t; NULL = the context's own stream) and returns without
+ * synchronising; kg_fetch() waits and returns the result. */
+int kg_launch_device(kg_ctx* ctx, const uint64_t* d_xbits, uint64_t n_kmers,
+                     uint32_t words_per_kmer, void* stream);
+int kg_fetch(kg_ctx* ctx, kg_result* res, kg_stats* stats);
+
+/* As kg_launch_device, and also computes the per-k-mer statistics that the
+ * next kg_fetch copies into its kg_stats (the reference keeps them only in
+ * memory, src/kgwas.cpp:156-158,248). */
+int kg_launch_device_stats(kg_ctx* ctx, const uint64_t* d_xbits, uint64_t n_kmers,
+                           uint32_t words_per_kmer, void* stream);
+
+/* Page-locked host memory for packed rows, so that kg_run_host copies at full
+ * link speed without staging; NULL on failure.  Free with kg_host_free. */
+void* kg_host_alloc(size_t bytes);
+void kg_host_free(void* p);
+
+/* Number of kernel launches the last kg_run_host / kg_launch_device made. */
+int kg_last_launch_count(const kg_ctx* ctx);
+
+const char* kg_last_error(const kg_ctx* ctx);
+void kg_destroy(kg_ctx* ctx);
+
+/* Library version string. */
+const char* kg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KGWAS_CUDA_H */

@@ -1,0 +1,100 @@
+"""In-tree build of the CUDA library and the ``kgwas`` program.
+
+Outputs (git-ignored, shipped with the source tree):
+  supergwas_b200/lib/libkgwas_cuda.so   C ABI of include/kgwas_cuda.h
+  supergwas_b200/bin/kgwas              drop-in for the reference's kgwas CLI
+
+Everything device-side is compiled for sm_100a only.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIB_DIR = os.path.join(PKG, "lib")
+BIN_DIR = os.path.join(PKG, "bin")
+LIB = os.path.join(LIB_DIR, "libkgwas_cuda.so")
+CLI = os.path.join(BIN_DIR, "kgwas")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+LIB_SOURCES = ["kernels.cu", "capi.cpp", "prep.cpp"]
+CLI_SOURCES = ["kgwas_main.cpp", "kgwas_io.cpp"]
+
+
+def nvcc() -> str:
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def _newer(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return False
+    t = os.path.getmtime(target)
+    return all(os.path.getmtime(d) <= t for d in deps)
+
+
+def _deps(names):
+    out = [os.path.join(CSRC, s) for s in names]
+    out += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".hpp", ".cuh", ".h"))]
+    out.append(os.path.join(ROOT, "include", "kgwas_cuda.h"))
+    out.append(os.path.abspath(__file__))
+    return out
+
+
+def run(cmd, verbose=False):
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError(f"build failed: {' '.join(cmd[:3])} ...")
+    return r
+
+
+def build_lib(force=False, verbose=False, ptxas_verbose=False) -> str:
+    deps = _deps(LIB_SOURCES)
+    if not force and _newer(LIB, deps):
+        return LIB
+    os.makedirs(LIB_DIR, exist_ok=True)
+    cmd = [nvcc(), *ARCH, "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3",
+           "-shared", "-o", LIB, *[os.path.join(CSRC, s) for s in LIB_SOURCES]]
+    if ptxas_verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    r = run(cmd, verbose)
+    if ptxas_verbose:
+        sys.stderr.write(r.stderr)
+    return LIB
+
+
+def build_cli(force=False, verbose=False) -> str:
+    deps = _deps(CLI_SOURCES) + [LIB]
+    if not force and _newer(CLI, deps):
+        return CLI
+    os.makedirs(BIN_DIR, exist_ok=True)
+    cmd = ["g++", "-O3", "-std=c++17", "-fopenmp", "-o", CLI,
+           *[os.path.join(CSRC, s) for s in CLI_SOURCES],
+           "-L" + LIB_DIR, "-lkgwas_cuda", "-Wl,-rpath,$ORIGIN/../lib", "-lz", "-lpthread"]
+    run(cmd, verbose)
+    return CLI
+
+
+def build_all(force=False, verbose=False):
+    build_lib(force, verbose)
+    build_cli(force, verbose)
+    return LIB, CLI
+
+
+if __name__ == "__main__":
+    force = "--force" in sys.argv
+    verbose = "-v" in sys.argv
+    if "--ptxas" in sys.argv:
+        build_lib(True, verbose, ptxas_verbose=True)
+    else:
+        print(build_all(force, verbose))

@@ -1,0 +1,508 @@
+// capi.cpp -- the C ABI of include/kgwas_cuda.h.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/kgwas_cuda.h"
+#include "kernels.hpp"
+#include "prep.hpp"
+
+#define KG_VERSION "kgwas-b200 0.1.0"
+
+namespace {
+
+constexpr int NBUF = 2;  // host-run chunk buffers in flight
+
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+}  // namespace
+
+struct kg_ctx {
+  kg_opts opts{};
+  int num_sms = 0;
+  cudaStream_t stream = nullptr, copy_stream = nullptr;
+  std::string err;
+  bool have_structure = false;
+  int n_row = 0;  // samples per packed row
+  kg::Prepared prep;
+  kg::LimbCols limbs;
+  kg::EpiParams P{};
+  kg::LimbMap LM{};
+  // structure on the device
+  double* dV = nullptr;
+  int cm = 0, nsteps = 0;
+  int8_t* dB = nullptr;
+  int nchunk = 0;
+  // outputs on the device
+  unsigned long long* dCounters = nullptr;
+  kg_hit* dHits = nullptr;
+  unsigned long long hit_cap = 0;
+  uint8_t* dTested = nullptr;
+  double* dStat[7] = {};
+  size_t stat_cap = 0;
+  // host result
+  std::vector<kg_hit> hits;
+  unsigned long long counters[3] = {0, 0, 0};
+  // pending device launch
+  bool pending = false;
+  const uint64_t* pend_x = nullptr;
+  uint64_t pend_m = 0;
+  uint32_t pend_wpk = 0;
+  bool pend_stats = false;
+  cudaStream_t pend_stream = nullptr;
+  int launches = 0;
+  // host-run buffers
+  uint64_t* dChunk[NBUF] = {};
+  void* hStage[NBUF] = {};
+  size_t chunk_bytes = 0;
+  cudaEvent_t ev_h2d[NBUF] = {}, ev_k[NBUF] = {};
+
+  int fail(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+  int cuda_fail(cudaError_t e, const char* what) {
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return KG_ERR_CUDA;
+  }
+};
+
+#define KG_CUDA(call, what)                              \
+  do {                                                   \
+    cudaError_t e__ = (call);                            \
+    if (e__ != cudaSuccess) return ctx->cuda_fail(e__, what); \
+  } while (0)
+
+extern "C" {
+
+const char* kg_version(void) { return KG_VERSION; }
+
+void kg_default_opts(kg_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->device = 0;
+  o->precision = KG_PREC_SPLIT_I8;
+  o->corr_threshold = 0.2;
+  o->log10_thresh = 6.0;
+  o->limbs_u = 3;
+  o->limbs_y = 5;
+}
+
+int kg_create(kg_ctx** out, const kg_opts* opts) {
+  if (!out) return KG_ERR_INVALID;
+  *out = nullptr;
+  kg_ctx* ctx = new (std::nothrow) kg_ctx();
+  if (!ctx) return KG_ERR_NOMEM;
+  if (opts) ctx->opts = *opts; else kg_default_opts(&ctx->opts);
+  if (ctx->opts.limbs_u == 0) ctx->opts.limbs_u = 3;
+  if (ctx->opts.limbs_y == 0) ctx->opts.limbs_y = 5;
+  if (ctx->opts.precision != KG_PREC_SPLIT_I8 && ctx->opts.precision != KG_PREC_FP64) {
+    delete ctx;
+    return KG_ERR_INVALID;
+  }
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ctx->opts.device < 0 || ctx->opts.device >= ndev) {
+    delete ctx;
+    return KG_ERR_CUDA;
+  }
+  if (cudaSetDevice(ctx->opts.device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->opts.device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc((void**)&ctx->dCounters, 4 * sizeof(unsigned long long)) != cudaSuccess) {
+    kg_destroy(ctx);
+    return KG_ERR_CUDA;
+  }
+  if (ctx->opts.precision == KG_PREC_SPLIT_I8) {
+    int cc_major = 0, cc_minor = 0;
+    cudaDeviceGetAttribute(&cc_major, cudaDevAttrComputeCapabilityMajor, ctx->opts.device);
+    cudaDeviceGetAttribute(&cc_minor, cudaDevAttrComputeCapabilityMinor, ctx->opts.device);
+    if (cc_major != 10 || cc_minor != 0) {
+      kg_destroy(ctx);
+      return KG_ERR_UNSUPPORTED;
+    }
+  }
+  for (int b = 0; b < NBUF; ++b) {
+    if (cudaEventCreateWithFlags(&ctx->ev_h2d[b], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_k[b], cudaEventDisableTiming) != cudaSuccess) {
+      kg_destroy(ctx);
+      return KG_ERR_CUDA;
+    }
+  }
+  *out = ctx;
+  return KG_OK;
+}
+
+void kg_destroy(kg_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->opts.device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+  dfree(ctx->dV);
+  dfree(ctx->dB);
+  dfree(ctx->dCounters);
+  dfree(ctx->dHits);
+  dfree(ctx->dTested);
+  for (auto& p : ctx->dStat) dfree(p);
+  for (int b = 0; b < NBUF; ++b) {
+    dfree(ctx->dChunk[b]);
+    if (ctx->hStage[b]) cudaFreeHost(ctx->hStage[b]);
+    if (ctx->ev_h2d[b]) cudaEventDestroy(ctx->ev_h2d[b]);
+    if (ctx->ev_k[b]) cudaEventDestroy(ctx->ev_k[b]);
+  }
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  delete ctx;
+}
+
+const char* kg_last_error(const kg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int kg_last_launch_count(const kg_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int kg_set_structure_ex(kg_ctx* ctx, const double* U, int n, int k, const double* y, const int32_t* sample_pos,
+                        int n_row_samples, double* yyM_out) {
+  if (!ctx) return KG_ERR_INVALID;
+  KG_CUDA(cudaSetDevice(ctx->opts.device), "cudaSetDevice");
+  ctx->have_structure = false;
+  const int n_row = sample_pos ? n_row_samples : n;
+  if (sample_pos) {
+    if (n_row_samples < n) return ctx->fail(KG_ERR_INVALID, "n_row_samples < n");
+    std::vector<char> seen((size_t)n_row_samples, 0);
+    for (int i = 0; i < n; ++i) {
+      if (sample_pos[i] < 0 || sample_pos[i] >= n_row_samples)
+        return ctx->fail(KG_ERR_INVALID, "sample_pos out of range");
+      if (seen[sample_pos[i]]++) return ctx->fail(KG_ERR_INVALID, "sample_pos has a repeated position");
+    }
+  }
+  std::string e = kg::prepare(U, n, k, y, ctx->prep);
+  if (!e.empty()) return ctx->fail(KG_ERR_INVALID, e);
+  const kg::Prepared& p = ctx->prep;
+  kg::EpiParams& P = ctx->P;
+  std::memset(&P, 0, sizeof(P));
+  P.n = n;
+  P.k = k;
+  P.b = p.b;
+  P.kappa = p.kappa;
+  P.yyM = p.yyM;
+  P.ynorm = p.ynorm;
+  P.corr_thr = ctx->opts.corr_threshold;
+  P.p_thresh = std::pow(10.0, -ctx->opts.log10_thresh);
+  for (int j = 0; j < k; ++j) {
+    P.a[j] = p.a[j];
+    P.g[j] = p.g[j];
+  }
+  if (yyM_out) *yyM_out = p.yyM;
+  ctx->n_row = n_row;
+  if (ctx->opts.precision == KG_PREC_FP64) {
+    // columns: [count, d_0 .. d_{k-1}, d_y], rows = packed-row sample positions
+    const int C = k + 2;
+    ctx->cm = kg::fp64_cm(C);
+    if (ctx->cm < 0) return ctx->fail(KG_ERR_UNSUPPORTED, "too many U.bin columns for the FP64 form");
+    ctx->nsteps = kg::fp64_steps(n_row);
+    std::vector<double> V((size_t)ctx->nsteps * 128 * ctx->cm, 0.0);
+    for (int i = 0; i < n; ++i) {
+      const size_t r = (size_t)(sample_pos ? sample_pos[i] : i) * ctx->cm;
+      V[r] = 1.0;
+      for (int j = 0; j <= k; ++j) V[r + 1 + j] = p.d[(size_t)j * n + i];
+    }
+    dfree(ctx->dV);
+    KG_CUDA(cudaMalloc((void**)&ctx->dV, V.size() * sizeof(double)), "cudaMalloc(V)");
+    KG_CUDA(cudaMemcpy(ctx->dV, V.data(), V.size() * sizeof(double), cudaMemcpyHostToDevice), "copy V");
+  } else {
+    e = kg::make_limbs(p, sample_pos, n_row, ctx->opts.limbs_u, ctx->opts.limbs_y, kg::tc_kc(), ctx->limbs);
+    if (!e.empty()) return ctx->fail(KG_ERR_UNSUPPORTED, e);
+    if (!kg::tc_supported_n(ctx->limbs.N))
+      return ctx->fail(KG_ERR_UNSUPPORTED, "contraction width N=" + std::to_string(ctx->limbs.N) +
+                                               " not supported by the tensor-core kernel");
+    std::vector<int8_t> img;
+    kg::make_b_image(ctx->limbs, kg::tc_kc(), img);
+    ctx->nchunk = ctx->limbs.Kpad / kg::tc_kc();
+    kg::LimbMap& LM = ctx->LM;
+    std::memset(&LM, 0, sizeof(LM));
+    LM.N = ctx->limbs.N;
+    LM.count_col = ctx->limbs.count_col;
+    for (int j = 0; j <= k; ++j) {
+      LM.first[j] = ctx->limbs.first[j];
+      LM.nl[j] = ctx->limbs.nl[j];
+      LM.scale[j] = ctx->limbs.scale[j];
+    }
+    dfree(ctx->dB);
+    KG_CUDA(cudaMalloc((void**)&ctx->dB, img.size()), "cudaMalloc(B)");
+    KG_CUDA(cudaMemcpy(ctx->dB, img.data(), img.size(), cudaMemcpyHostToDevice), "copy B");
+  }
+  ctx->have_structure = true;
+  return KG_OK;
+}
+
+int kg_set_structure(kg_ctx* ctx, const double* U, int n, int k, const double* y, double* yyM_out) {
+  return kg_set_structure_ex(ctx, U, n, k, y, nullptr, n, yyM_out);
+}
+
+}  // extern "C"
+
+namespace {
+
+int ensure_hits(kg_ctx* ctx, unsigned long long cap) {
+  if (ctx->hit_cap >= cap && ctx->dHits) return KG_OK;
+  dfree(ctx->dHits);
+  ctx->hit_cap = 0;
+  KG_CUDA(cudaMalloc((void**)&ctx->dHits, cap * sizeof(kg_hit)), "cudaMalloc(hits)");
+  ctx->hit_cap = cap;
+  return KG_OK;
+}
+
+int ensure_stats(kg_ctx* ctx, size_t m) {
+  if (ctx->stat_cap >= m && ctx->dTested) return KG_OK;
+  dfree(ctx->dTested);
+  for (auto& p : ctx->dStat) dfree(p);
+  ctx->stat_cap = 0;
+  KG_CUDA(cudaMalloc((void**)&ctx->dTested, std::max<size_t>(m, 1)), "cudaMalloc(stats)");
+  for (auto& p : ctx->dStat) KG_CUDA(cudaMalloc((void**)&p, std::max<size_t>(m, 1) * sizeof(double)), "cudaMalloc(stats)");
+  ctx->stat_cap = m;
+  return KG_OK;
+}
+
+int check_shape(kg_ctx* ctx, const void* x, uint64_t m, uint32_t wpk) {
+  if (!ctx->have_structure) return ctx->fail(KG_ERR_STATE, "kg_set_structure has not succeeded");
+  if (m > 0 && !x) return ctx->fail(KG_ERR_INVALID, "xbits is NULL");
+  if (wpk == 0 || (wpk & 1u)) return ctx->fail(KG_ERR_INVALID, "words_per_kmer must be even and > 0");
+  if ((uint64_t)wpk * 64 < (uint64_t)ctx->n_row)
+    return ctx->fail(KG_ERR_INVALID, "words_per_kmer*64 < samples per row");
+  return KG_OK;
+}
+
+int launch_one(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, uint64_t offset, bool stats,
+               cudaStream_t st) {
+  if (m == 0) return KG_OK;
+  kg::DevOut O{};
+  O.counters = ctx->dCounters;
+  O.hits = ctx->dHits;
+  O.hit_cap = ctx->hit_cap;
+  O.kmer_offset = offset;
+  if (stats) {
+    O.tested = ctx->dTested;
+    O.chisq = ctx->dStat[0];
+    O.pval = ctx->dStat[1];
+    O.effect = ctx->dStat[2];
+    O.mlog10p = ctx->dStat[3];
+    O.xxM = ctx->dStat[4];
+    O.xyM = ctx->dStat[5];
+    O.cor = ctx->dStat[6];
+  }
+  cudaError_t e;
+  if (ctx->opts.precision == KG_PREC_FP64) {
+    kg::LaunchFp64 L{dx, m, (int)wpk, ctx->dV, ctx->nsteps, ctx->cm, &ctx->P, &O, ctx->num_sms};
+    e = kg::launch_fp64(L, st);
+  } else {
+    kg::LaunchTc L{dx, m, (int)wpk, ctx->nchunk, ctx->dB, &ctx->P, &ctx->LM, &O, ctx->num_sms};
+    e = kg::launch_tc(L, st);
+  }
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "kernel launch");
+  ++ctx->launches;
+  return KG_OK;
+}
+
+int collect(kg_ctx* ctx, uint64_t m, kg_result* res, kg_stats* st, bool stats_on_device) {
+  if (ctx->counters[2] & ~(unsigned long long)kg::ERR_HIT_OVERFLOW)
+    return ctx->fail(KG_ERR_TIMEOUT, "a bounded device-side wait gave up (error bits " +
+                                         std::to_string(ctx->counters[2]) + ")");
+  const unsigned long long nh = ctx->counters[1];
+  ctx->hits.resize(nh);
+  if (nh) {
+    KG_CUDA(cudaMemcpy(ctx->hits.data(), ctx->dHits, nh * sizeof(kg_hit), cudaMemcpyDeviceToHost), "copy hits");
+    std::sort(ctx->hits.begin(), ctx->hits.end(), [](const kg_hit& a, const kg_hit& b) { return a.kmer < b.kmer; });
+  }
+  if (st && stats_on_device && m) {
+    if (st->tested) KG_CUDA(cudaMemcpy(st->tested, ctx->dTested, m, cudaMemcpyDeviceToHost), "copy stats");
+    double* outs[7] = {st->chisq, st->pval, st->effect, st->mlog10p, st->xxM, st->xyM, st->cor};
+    for (int i = 0; i < 7; ++i)
+      if (outs[i]) KG_CUDA(cudaMemcpy(outs[i], ctx->dStat[i], m * sizeof(double), cudaMemcpyDeviceToHost), "copy stats");
+  }
+  if (res) {
+    res->n_kmers = m;
+    res->n_tested = ctx->counters[0];
+    res->n_hits = nh;
+    res->hits = ctx->hits.data();
+  }
+  return KG_OK;
+}
+
+bool want_stats(const kg_stats* st) {
+  return st && (st->tested || st->chisq || st->pval || st->effect || st->mlog10p || st->xxM || st->xyM || st->cor);
+}
+
+void par_memcpy(void* dst, const void* src, size_t bytes) {
+  const size_t kMin = (size_t)64 << 20;
+  unsigned nt = std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
+  if (bytes < kMin || nt == 1) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t per = (bytes + nt - 1) / nt;
+  for (unsigned t = 0; t < nt; ++t) {
+    const size_t a = t * per, b = std::min(bytes, a + per);
+    if (a >= b) break;
+    th.emplace_back([=] { std::memcpy((char*)dst + a, (const char*)src + a, b - a); });
+  }
+  for (auto& t : th) t.join();
+}
+
+int run_host_once(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t wpk, bool stats) {
+  const size_t row = (size_t)wpk * 8;
+  size_t want = (size_t)512 << 20;
+  if (const char* v = std::getenv("KG_CHUNK_MB")) want = (size_t)std::max(1, std::atoi(v)) << 20;
+  uint64_t per = std::max<uint64_t>(1, want / row);
+  if (per > m) per = m;
+  const size_t bytes = (size_t)per * row;
+  cudaPointerAttributes attr{};
+  bool pinned = cudaPointerGetAttributes(&attr, xbits) == cudaSuccess &&
+                (attr.type == cudaMemoryTypeHost || attr.type == cudaMemoryTypeManaged);
+  cudaGetLastError();
+  if (ctx->chunk_bytes < bytes) {
+    for (int b = 0; b < NBUF; ++b) {
+      dfree(ctx->dChunk[b]);
+      if (ctx->hStage[b]) cudaFreeHost(ctx->hStage[b]);
+      ctx->hStage[b] = nullptr;
+    }
+    ctx->chunk_bytes = 0;
+    for (int b = 0; b < NBUF; ++b) KG_CUDA(cudaMalloc((void**)&ctx->dChunk[b], bytes), "cudaMalloc(chunk)");
+    ctx->chunk_bytes = bytes;
+  }
+  if (!pinned)
+    for (int b = 0; b < NBUF; ++b)
+      if (!ctx->hStage[b]) KG_CUDA(cudaHostAlloc(&ctx->hStage[b], ctx->chunk_bytes, cudaHostAllocDefault), "cudaHostAlloc");
+  KG_CUDA(cudaMemsetAsync(ctx->dCounters, 0, 4 * sizeof(unsigned long long), ctx->stream), "memset");
+  const uint64_t nch = (m + per - 1) / per;
+  for (uint64_t i = 0; i < nch; ++i) {
+    const int b = (int)(i % NBUF);
+    const uint64_t s = i * per, cnt = std::min<uint64_t>(per, m - s);
+    const size_t nb = (size_t)cnt * row;
+    const char* src = (const char*)xbits + (size_t)s * row;
+    if (i >= (uint64_t)NBUF) {
+      // buffer b was last read by chunk i-NBUF's copy and kernel
+      KG_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_k[b], 0), "wait");
+      if (!pinned) KG_CUDA(cudaEventSynchronize(ctx->ev_h2d[b]), "sync");
+    }
+    if (!pinned) {
+      par_memcpy(ctx->hStage[b], src, nb);
+      src = (const char*)ctx->hStage[b];
+    }
+    KG_CUDA(cudaMemcpyAsync(ctx->dChunk[b], src, nb, cudaMemcpyHostToDevice, ctx->copy_stream), "H2D");
+    KG_CUDA(cudaEventRecord(ctx->ev_h2d[b], ctx->copy_stream), "record");
+    KG_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_h2d[b], 0), "wait");
+    int rc = launch_one(ctx, ctx->dChunk[b], cnt, wpk, s, stats, ctx->stream);
+    if (rc) return rc;
+    KG_CUDA(cudaEventRecord(ctx->ev_k[b], ctx->stream), "record");
+  }
+  KG_CUDA(cudaMemcpyAsync(ctx->counters, ctx->dCounters, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                          ctx->stream),
+          "copy counters");
+  KG_CUDA(cudaStreamSynchronize(ctx->stream), "kernel");
+  return KG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kg_run_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t wpk, kg_result* res, kg_stats* st) {
+  if (!ctx) return KG_ERR_INVALID;
+  KG_CUDA(cudaSetDevice(ctx->opts.device), "cudaSetDevice");
+  int rc = check_shape(ctx, xbits, m, wpk);
+  if (rc) return rc;
+  ctx->pending = false;
+  ctx->launches = 0;
+  const bool stats = want_stats(st);
+  if (stats && (rc = ensure_stats(ctx, m))) return rc;
+  if ((rc = ensure_hits(ctx, std::max<unsigned long long>(ctx->hit_cap, 1ull << 16)))) return rc;
+  std::memset(ctx->counters, 0, sizeof(ctx->counters));
+  if (m) {
+    if ((rc = run_host_once(ctx, xbits, m, wpk, stats))) return rc;
+    if (ctx->counters[2] & kg::ERR_HIT_OVERFLOW) {
+      if ((rc = ensure_hits(ctx, ctx->counters[1]))) return rc;
+      if ((rc = run_host_once(ctx, xbits, m, wpk, stats))) return rc;
+    }
+  }
+  return collect(ctx, m, res, st, stats);
+}
+
+int kg_launch_device(kg_ctx* ctx, const uint64_t* d_x, uint64_t m, uint32_t wpk, void* stream) {
+  if (!ctx) return KG_ERR_INVALID;
+  KG_CUDA(cudaSetDevice(ctx->opts.device), "cudaSetDevice");
+  int rc = check_shape(ctx, d_x, m, wpk);
+  if (rc) return rc;
+  if ((rc = ensure_hits(ctx, std::max<unsigned long long>(ctx->hit_cap, 1ull << 16)))) return rc;
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  ctx->launches = 0;
+  KG_CUDA(cudaMemsetAsync(ctx->dCounters, 0, 4 * sizeof(unsigned long long), st), "memset");
+  if ((rc = launch_one(ctx, d_x, m, wpk, 0, ctx->pend_stats, st))) return rc;
+  ctx->pending = true;
+  ctx->pend_x = d_x;
+  ctx->pend_m = m;
+  ctx->pend_wpk = wpk;
+  ctx->pend_stream = st;
+  return KG_OK;
+}
+
+}  // extern "C"
+
+// Per-k-mer statistics for device launches are switched on by this
+// internal entry (used by kg_fetch's caller through kg_launch_device_stats).
+extern "C" int kg_launch_device_stats(kg_ctx* ctx, const uint64_t* d_x, uint64_t m, uint32_t wpk, void* stream) {
+  if (!ctx) return KG_ERR_INVALID;
+  int rc = ensure_stats(ctx, m);
+  if (rc) return rc;
+  ctx->pend_stats = true;
+  rc = kg_launch_device(ctx, d_x, m, wpk, stream);
+  if (rc) ctx->pend_stats = false;
+  return rc;
+}
+
+extern "C" void* kg_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, bytes ? bytes : 1, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+extern "C" void kg_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+
+extern "C" int kg_fetch(kg_ctx* ctx, kg_result* res, kg_stats* st) {
+  if (!ctx) return KG_ERR_INVALID;
+  if (!ctx->pending) return ctx->fail(KG_ERR_STATE, "kg_fetch without a pending kg_launch_device");
+  KG_CUDA(cudaSetDevice(ctx->opts.device), "cudaSetDevice");
+  ctx->pending = false;
+  const bool stats = ctx->pend_stats;
+  ctx->pend_stats = false;
+  KG_CUDA(cudaMemcpyAsync(ctx->counters, ctx->dCounters, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                          ctx->pend_stream),
+          "copy counters");
+  KG_CUDA(cudaStreamSynchronize(ctx->pend_stream), "kernel");
+  if (ctx->counters[2] & kg::ERR_HIT_OVERFLOW) {
+    int rc = ensure_hits(ctx, ctx->counters[1]);
+    if (rc) return rc;
+    KG_CUDA(cudaMemsetAsync(ctx->dCounters, 0, 4 * sizeof(unsigned long long), ctx->pend_stream), "memset");
+    if ((rc = launch_one(ctx, ctx->pend_x, ctx->pend_m, ctx->pend_wpk, 0, stats, ctx->pend_stream))) return rc;
+    KG_CUDA(cudaMemcpyAsync(ctx->counters, ctx->dCounters, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            ctx->pend_stream),
+            "copy counters");
+    KG_CUDA(cudaStreamSynchronize(ctx->pend_stream), "kernel");
+  }
+  return collect(ctx, ctx->pend_m, res, st, stats);
+}

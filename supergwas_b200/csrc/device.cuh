@@ -1,0 +1,215 @@
+// device.cuh -- parameters, PTX helpers and the shared FP64 epilogue of the
+// association kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "params.hpp"
+
+namespace kg {
+
+// A bounded wait gives up after this long and reports KG_ERR_TIMEOUT.
+constexpr unsigned long long WAIT_LIMIT_NS = 2000000000ull;
+
+__device__ __forceinline__ unsigned long long gtimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// ---------------------------------------------------------------- mbarrier
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: false (and an error bit in counters[2]) after WAIT_LIMIT_NS.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
+                                          unsigned long long* counters, unsigned code) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = gtimer_ns();
+  while (!mbar_try(bar, parity)) {
+    if (gtimer_ns() - t0 > WAIT_LIMIT_NS) {
+      atomicOr(counters + 2, (unsigned long long)code);
+      return false;
+    }
+  }
+  return true;
+}
+
+// ----------------------------------------------------------- bulk copies
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// ---------------------------------------------------------------- tcgen05
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+// D[tmem] (+)= A[smem desc] * B[smem desc], kind::i8, int32 accumulate.
+__device__ __forceinline__ void tc_mma_i8_ss(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                             uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+// D[tmem] (+)= A[tmem] * B[smem desc], kind::i8.
+__device__ __forceinline__ void tc_mma_i8_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
+                                             uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// 32 lanes x 32-bit, 16 consecutive columns per thread.
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+// 32 lanes x 32-bit, 8 consecutive columns per thread.
+__device__ __forceinline__ void tc_st8(uint32_t taddr, const uint32_t (&r)[8]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(r[0]),
+               "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+               : "memory");
+}
+
+// Shared-memory matrix descriptor, K-major, no swizzle (core matrix = 8 rows
+// x 16 bytes contiguous); lbo = byte distance of K-adjacent core matrices,
+// sbo = byte distance of M/N-adjacent 8-row groups.
+__device__ __forceinline__ uint64_t sdesc_noswz(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  return d;               // base offset 0, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor: kind::i8, s8 x s8 -> s32, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// ---------------------------------------------------------------- epilogue
+// -log10 erfc(z) without underflow (log-domain tail through erfcx).
+__device__ __forceinline__ double mlog10_sf(double T) {
+  if (!(T > 0.0)) return 0.0;
+  const double z = sqrt(0.5 * T);
+  if (z < 5.0) return -log10(erfc(z));
+  return (z * z - log(erfcx(z))) * 0.43429448190325182765;
+}
+
+// Statistics and outputs of one k-mer, given c = popcount(x),
+// ss = sum_j s_j^2, gs = sum_j g_j e_j, ey = d_y . x.  Must be called by
+// all 32 lanes of a warp (warp-aggregated atomics).
+__device__ __forceinline__ void finish_kmer(const EpiParams& P, const DevOut& O, unsigned long long local,
+                                            bool valid, int c, double ss, double gs, double ey) {
+  const int n = P.n;
+  bool tested = valid && c > 0 && c < n && !(P.ynorm < 1e-12);
+  double cor = 0.0;
+  if (tested) {
+    const double xcn2 = (double)c * (double)(n - c) / (double)n;  // ||x - mean x||^2
+    const double xyc = ey + gs + P.kappa * (double)c;              // x . (y - mean y)
+    cor = xyc / (sqrt(xcn2) * P.ynorm);
+    tested = !(fabs(cor) < P.corr_thr);                             // src/kgwas.cpp:199,467
+  }
+  double xxM = 0, xyM = 0, effect = 0, T = 0, p = 1;
+  if (tested) {
+    xxM = (double)c - ss;
+    xyM = P.b * (double)c + ey;
+    // compute_hit, src/kgwas.cpp:44-56
+    const double eps = 1e-12;
+    if (xxM > eps && P.yyM > eps) {
+      double r2 = (xyM * xyM) / (xxM * P.yyM);
+      if (r2 < 0) r2 = 0;
+      if (r2 >= 1) r2 = 1 - 1e-15;
+      T = (double)n * log(1.0 / (1.0 - r2));
+      p = erfc(sqrt(0.5 * T));
+      effect = xyM / (xxM * P.yyM);
+    }
+  }
+  const bool hit = tested && p <= P.p_thresh;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned tmask = __ballot_sync(0xffffffffu, tested);
+  if (lane == 0 && tmask) atomicAdd(O.counters + 0, (unsigned long long)__popc(tmask));
+  const unsigned hmask = __ballot_sync(0xffffffffu, hit);
+  if (hmask) {
+    unsigned long long base = 0;
+    const int leader = __ffs(hmask) - 1;
+    if ((int)lane == leader) base = atomicAdd(O.counters + 1, (unsigned long long)__popc(hmask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (hit) {
+      const unsigned long long slot = base + __popc(hmask & ((1u << lane) - 1u));
+      if (slot < O.hit_cap) {
+        kg_hit h;
+        h.kmer = O.kmer_offset + local;
+        h.effect = effect;
+        h.pval = p;
+        h.chisq = T;
+        O.hits[slot] = h;
+      } else {
+        atomicOr(O.counters + 2, (unsigned long long)ERR_HIT_OVERFLOW);
+      }
+    }
+  }
+  if (valid && O.tested) {
+    const unsigned long long g = O.kmer_offset + local;
+    O.tested[g] = tested ? 1 : 0;
+    O.chisq[g] = T;
+    O.pval[g] = p;
+    O.effect[g] = effect;
+    O.mlog10p[g] = tested ? mlog10_sf(T) : 0.0;
+    O.xxM[g] = xxM;
+    O.xyM[g] = xyM;
+    O.cor[g] = cor;
+  }
+}
+
+}  // namespace kg

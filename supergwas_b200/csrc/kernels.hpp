@@ -1,0 +1,40 @@
+// kernels.hpp -- host-side launch interface of the association kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "params.hpp"
+
+namespace kg {
+
+struct LaunchFp64 {
+  const uint64_t* x;          // packed rows (device)
+  unsigned long long m;       // k-mers in this launch
+  int wpk;                    // words per k-mer
+  const double* V;            // nsteps*128 x cm FP64, sample-major, zero padded (device)
+  int nsteps, cm;             // sample steps of 128; padded column count
+  const EpiParams* P;
+  const DevOut* O;
+  int num_sms;
+};
+
+struct LaunchTc {
+  const uint64_t* x;
+  unsigned long long m;
+  int wpk;
+  int nchunk;                 // K chunks of tc_kc() samples
+  const int8_t* Bimg;         // B operand shared-memory image, chunk after chunk (device)
+  const EpiParams* P;
+  const LimbMap* LM;
+  const DevOut* O;
+  int num_sms;
+};
+
+int fp64_cm(int C);           // padded column count for C contraction columns (-1: too many)
+int fp64_steps(int n);        // 128-sample steps covering n samples
+cudaError_t launch_fp64(const LaunchFp64& L, cudaStream_t st);
+
+int tc_kc();                  // samples per K chunk of the tensor-core kernel
+bool tc_supported_n(int N);
+cudaError_t launch_tc(const LaunchTc& L, cudaStream_t st);
+
+}  // namespace kg

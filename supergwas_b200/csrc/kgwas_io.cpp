@@ -1,0 +1,424 @@
+// kgwas_io.cpp -- see kgwas_io.hpp.
+#include "kgwas_io.hpp"
+
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+#include <zlib.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <memory>
+
+#include <omp.h>
+
+namespace kgio {
+
+void die(const std::string& m) {
+  std::cerr << "[ERROR] " << m << "\n";
+  std::exit(1);
+}
+
+void warn(const std::string& m) { std::cerr << "[WARN] " << m << "\n"; }
+
+int env_int(const char* k, int dflt) {
+  const char* v = std::getenv(k);
+  if (!v || !*v) return dflt;
+  try {
+    return std::max(1, std::stoi(v));
+  } catch (...) {
+    return dflt;
+  }
+}
+
+static double now_s() {
+  using clk = std::chrono::steady_clock;
+  return std::chrono::duration<double>(clk::now().time_since_epoch()).count();
+}
+Timer::Timer() : t0(now_s()) {}
+double Timer::sec() const { return now_s() - t0; }
+
+std::vector<std::string> load_lines(const std::string& file) {
+  std::ifstream in(file);
+  if (!in) die("open: " + file);
+  std::vector<std::string> v;
+  std::string s;
+  while (std::getline(in, s))
+    if (!s.empty()) {
+      if (s.back() == '\r') s.pop_back();
+      v.push_back(s);
+    }
+  return v;
+}
+
+std::unordered_map<std::string, double> load_pheno(const std::string& file) {
+  std::ifstream in(file);
+  if (!in) die("open: " + file);
+  std::unordered_map<std::string, double> m;
+  std::string id;
+  double val;
+  while (in >> id >> val) m[id] = val;
+  return m;
+}
+
+Overlap build_overlap(const std::string& samples_file, const std::string& pheno_file) {
+  Timer t;
+  Overlap ov;
+  ov.samples = load_lines(samples_file);
+  const int L = (int)ov.samples.size();
+  if (L <= 0) die("samples empty");
+  auto ph = load_pheno(pheno_file);
+  for (int j = 0; j < L; ++j) {
+    auto it = ph.find(ov.samples[j]);
+    if (it != ph.end()) {
+      ov.idxs.push_back(j);
+      ov.y.push_back(it->second);
+    }
+  }
+  if (ov.idxs.empty()) die("no phenotype overlap");
+  std::cerr << "[INFO] n=" << ov.y.size() << " (overlap)  (" << t.sec() << " s)\n";
+  return ov;
+}
+
+UData load_ubin(const std::string& path, int n) {
+  Timer t;
+  std::ifstream uin(path, std::ios::binary);
+  if (!uin) die("open: " + path);
+  int n_u = 0, r = 0;
+  uin.read((char*)&n_u, sizeof(int));
+  uin.read((char*)&r, sizeof(int));
+  if (!uin) die("short U.bin header");
+  if (n_u != n) die("U.bin n mismatch: file n=" + std::to_string(n_u) + " vs overlap n=" + std::to_string(n));
+  if (r < 0) die("short U.bin body");
+  UData ud;
+  ud.n = n;
+  ud.k = r;
+  ud.U.resize((size_t)n * r);
+  uin.read((char*)ud.U.data(), (std::streamsize)(sizeof(double) * (size_t)n * r));
+  if (!uin) die("short U.bin body");
+  std::cerr << "[INFO] loaded U (n=" << n << ", r=" << r << ")  (" << t.sec() << " s)\n";
+  return ud;
+}
+
+static bool file_exists(const std::string& p) {
+  struct stat st {};
+  return ::stat(p.c_str(), &st) == 0 && S_ISREG(st.st_mode);
+}
+
+static size_t probe_N_txt(const std::string& path) {
+  int fd = ::open(path.c_str(), O_RDONLY);
+  if (fd < 0) die("open: " + path);
+  struct stat st {};
+  if (fstat(fd, &st) != 0) {
+    ::close(fd);
+    die("fstat: " + path);
+  }
+  const size_t sz = (size_t)st.st_size;
+  if (sz == 0) {
+    ::close(fd);
+    die("empty: " + path);
+  }
+  void* p = mmap(nullptr, sz, PROT_READ, MAP_PRIVATE, fd, 0);
+  if (p == MAP_FAILED) {
+    ::close(fd);
+    die("mmap: " + path);
+  }
+  const char* b = (const char*)p;
+  const void* nl = memchr(b, '\n', sz);
+  const size_t N = nl ? (size_t)((const char*)nl - b) : sz;
+  munmap(p, sz);
+  ::close(fd);
+  if (N == 0) die("no bytes before newline: " + path);
+  return N;
+}
+
+static size_t probe_N_gz(const std::string& path) {
+  gzFile f = gzopen(path.c_str(), "rb");
+  if (!f) die("gzopen: " + path);
+  gzbuffer(f, 1 << 20);
+  const size_t CHUNK = 1 << 20;
+  std::unique_ptr<unsigned char[]> buf(new unsigned char[CHUNK]);
+  size_t total = 0;
+  for (;;) {
+    int n = gzread(f, buf.get(), (unsigned)CHUNK);
+    if (n < 0) {
+      int err = 0;
+      const char* msg = gzerror(f, &err);
+      gzclose(f);
+      die(std::string("gzread error: ") + (msg ? msg : ""));
+    }
+    if (n == 0) break;
+    const void* nl = memchr(buf.get(), '\n', (size_t)n);
+    if (nl) {
+      total += (size_t)((const unsigned char*)nl - buf.get());
+      gzclose(f);
+      return total;
+    }
+    total += (size_t)n;
+  }
+  gzclose(f);
+  if (total == 0) die("empty gz column: " + path);
+  return total;
+}
+
+static std::string col_name(int idx) {
+  char base[64];
+  std::snprintf(base, sizeof(base), "col_%06d.txt", idx);
+  return base;
+}
+
+size_t infer_N_from_bits(const std::string& bits_dir, int first_idx) {
+  Timer t;
+  const std::string p_txt = bits_dir + "/" + col_name(first_idx);
+  const std::string p_gz = p_txt + ".gz";
+  size_t N = 0;
+  const bool txt = file_exists(p_txt);
+  if (txt) N = probe_N_txt(p_txt);
+  else if (file_exists(p_gz)) N = probe_N_gz(p_gz);
+  else die("missing column: " + p_txt + " (and " + p_gz + ")");
+  if (N == 0) die("N=0");
+  std::cerr << "[INFO] inferred N=" << N << " rows  (" << t.sec() << " s)" << (txt ? " [from .txt]" : " [from .txt.gz]")
+            << "\n";
+  return N;
+}
+
+std::vector<std::string> load_kmers(const std::string& path, size_t N) {
+  std::vector<std::string> kmers;
+  kmers.reserve(N);
+  const bool gz = path.size() >= 3 && path.compare(path.size() - 3, 3, ".gz") == 0;
+  if (gz) {
+    gzFile f = gzopen(path.c_str(), "rb");
+    if (!f) die("gzopen: " + path);
+    const int BUFSZ = 1 << 15;
+    std::unique_ptr<char[]> buf(new char[BUFSZ]);
+    std::string line;
+    while (kmers.size() < N) {
+      char* r = gzgets(f, buf.get(), BUFSZ);
+      if (!r) {
+        int err = 0;
+        const char* msg = gzerror(f, &err);
+        if (err == Z_STREAM_END) break;
+        if (err != Z_OK) {
+          gzclose(f);
+          die(std::string("gzgets error: ") + (msg ? msg : ""));
+        }
+        break;
+      }
+      char* nl = strchr(r, '\n');
+      if (nl) {
+        *nl = '\0';
+        line.append(r);
+        kmers.push_back(std::move(line));
+        line.clear();
+      } else {
+        line.append(r);
+      }
+    }
+    gzclose(f);
+  } else {
+    std::ifstream in(path);
+    if (!in) die("open: " + path);
+    std::string s;
+    while (kmers.size() < N && std::getline(in, s)) {
+      if (!s.empty() && s.back() == '\r') s.pop_back();
+      kmers.push_back(std::move(s));
+    }
+  }
+  if (kmers.size() != N)
+    die("kmers lines != N (got " + std::to_string(kmers.size()) + ", expected " + std::to_string(N) + ")");
+  return kmers;
+}
+
+static void read_gz_exact_N(const std::string& path, unsigned char* dst, size_t N) {
+  gzFile f = gzopen(path.c_str(), "rb");
+  if (!f) die("gzopen: " + path);
+  gzbuffer(f, 1 << 20);
+  size_t got = 0;
+  while (got < N) {
+    int n = gzread(f, dst + got, (unsigned)std::min<size_t>(N - got, 1 << 20));
+    if (n <= 0) {
+      int err = 0;
+      const char* msg = gzerror(f, &err);
+      gzclose(f);
+      if (err == Z_STREAM_END)
+        die("short gz column: " + path + " (got " + std::to_string(got) + " < N " + std::to_string(N) + ")");
+      die(std::string("gzread error: ") + (msg ? msg : ""));
+    }
+    got += (size_t)n;
+  }
+  unsigned char extra;
+  int n = gzread(f, &extra, 1);
+  if (n == 1 && extra != '\n') {
+    gzclose(f);
+    die("gz column longer than expected (N+ extra non-newline): " + path);
+  }
+  gzclose(f);
+}
+
+namespace {
+struct Column {
+  const unsigned char* p = nullptr;
+  void* map = nullptr;
+  size_t map_sz = 0;
+  std::unique_ptr<unsigned char[]> buf;
+};
+}  // namespace
+
+void load_matrix_packed(const std::string& bits_dir, const std::vector<int>& idxs, size_t N, int threads,
+                        uint64_t* out) {
+  Timer t;
+  const int n = (int)idxs.size();
+  const uint32_t W = words_per_kmer(n);
+  std::vector<Column> cols(n);
+  std::atomic<int> done{0};
+  omp_set_num_threads(std::max(1, threads));
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int k = 0; k < n; ++k) {
+    const std::string p_txt = bits_dir + "/" + col_name(idxs[k]);
+    const std::string p_gz = p_txt + ".gz";
+    Column& c = cols[k];
+    if (file_exists(p_txt)) {
+      int fd = ::open(p_txt.c_str(), O_RDONLY);
+      if (fd < 0) die("open: " + p_txt);
+      struct stat st {};
+      if (fstat(fd, &st) != 0) {
+        ::close(fd);
+        die("fstat: " + p_txt);
+      }
+      const size_t sz = (size_t)st.st_size;
+      if (sz < N) {
+        ::close(fd);
+        die("short column: " + p_txt + " (size " + std::to_string(sz) + " < N " + std::to_string(N) + ")");
+      }
+      void* p = mmap(nullptr, sz, PROT_READ, MAP_PRIVATE, fd, 0);
+      ::close(fd);
+      if (p == MAP_FAILED) die("mmap: " + p_txt);
+      madvise(p, sz, MADV_SEQUENTIAL);
+      c.map = p;
+      c.map_sz = sz;
+      c.p = (const unsigned char*)p;
+    } else if (file_exists(p_gz)) {
+      c.buf.reset(new unsigned char[N]);
+      read_gz_exact_N(p_gz, c.buf.get(), N);
+      c.p = c.buf.get();
+    } else {
+      die("missing column: " + p_txt + " (and " + p_gz + ")");
+    }
+    const int d = ++done;
+    if ((d % 8) == 0) {
+#pragma omp critical
+      std::cerr << "\r[LOAD] " << d << "/" << n << std::flush;
+    }
+  }
+  // Transpose 64 sample columns at a time into one word column.
+  const size_t BLK = 8192;
+  const size_t nblk = (N + BLK - 1) / BLK;
+#pragma omp parallel
+  {
+    std::vector<uint64_t> acc(BLK);
+#pragma omp for schedule(static)
+    for (size_t b = 0; b < nblk; ++b) {
+      const size_t j0 = b * BLK, len = std::min(BLK, N - j0);
+      for (uint32_t wc = 0; wc < W; ++wc) {
+        std::fill(acc.begin(), acc.begin() + len, 0ull);
+        for (int tt = 0; tt < 64; ++tt) {
+          const int s = (int)wc * 64 + tt;
+          if (s >= n) break;
+          const unsigned char* src = cols[s].p + j0;
+          for (size_t jj = 0; jj < len; ++jj) acc[jj] |= (uint64_t)(src[jj] & 1u) << tt;
+        }
+        for (size_t jj = 0; jj < len; ++jj) out[(j0 + jj) * W + wc] = acc[jj];
+      }
+    }
+  }
+  for (auto& c : cols)
+    if (c.map) munmap(c.map, c.map_sz);
+  std::cerr << "\r[LOAD] " << n << "/" << n << "  (" << t.sec() << " s, LOAD_THREADS=" << threads << ")\n";
+}
+
+// ------------------------------------------------------------ ROWS reader
+RowsReader::RowsReader(const std::string& path) {
+  const bool gzm = path.size() >= 3 && path.compare(path.size() - 3, 3, ".gz") == 0;
+  if (gzm) {
+    gzFile f = gzopen(path.c_str(), "rb");
+    if (!f) die("Cannot open gz file: " + path);
+    gzbuffer(f, 1u << 20);
+    gz = f;
+  } else {
+    auto* in = new std::ifstream(path);
+    if (!*in) {
+      delete in;
+      die("Cannot open kmer file: " + path);
+    }
+    plain = in;
+  }
+}
+
+RowsReader::~RowsReader() {
+  if (gz) gzclose((gzFile)gz);
+  delete (std::ifstream*)plain;
+}
+
+// src/kgwas.cpp:318-341 for gz input (drops one '\r' before '\n'),
+// std::getline for plain input.
+bool RowsReader::next_line(std::string& out) {
+  if (plain) return (bool)std::getline(*(std::ifstream*)plain, out);
+  out.clear();
+  static thread_local std::unique_ptr<char[]> buf(new char[1u << 20]);
+  bool got_any = false;
+  for (;;) {
+    char* res = gzgets((gzFile)gz, buf.get(), (int)(1u << 20));
+    if (!res) return got_any;
+    got_any = true;
+    size_t len = std::strlen(res);
+    if (len == 0) continue;
+    if (res[len - 1] == '\n') {
+      size_t end = len - 1;
+      if (end > 0 && res[end - 1] == '\r') --end;
+      out.append(res, res + end);
+      return true;
+    }
+    out.append(res, res + len);
+  }
+}
+
+size_t RowsReader::read(size_t max_rows, const std::vector<int>& idxs, std::vector<std::string>& kmers,
+                        std::vector<uint64_t>& packed) {
+  const int n = (int)idxs.size();
+  const uint32_t W = words_per_kmer(n);
+  std::string line;
+  size_t got = 0;
+  while (got < max_rows && next_line(line)) {
+    if (line.empty()) continue;
+    ++lines;
+    size_t tab = line.find('\t');
+    if (tab == std::string::npos) {
+      tab = line.find(' ');
+      if (tab == std::string::npos) continue;
+    }
+    const size_t nb = line.size() - (tab + 1);
+    const char* bits = line.data() + tab + 1;
+    const size_t base = packed.size();
+    packed.resize(base + W, 0ull);
+    for (int j = 0; j < n; ++j) {
+      const size_t pos = (size_t)idxs[j];
+      char c;
+      if (pos < nb) c = bits[pos];
+      else if (pos == nb) c = '\0';  // std::string::operator[] at size()
+      else die("bitstring shorter than the samples list in row: " + line.substr(0, tab));
+      if (c == '1') packed[base + (size_t)(j >> 6)] |= 1ull << (j & 63);
+    }
+    kmers.emplace_back(line, 0, tab);
+    ++got;
+  }
+  return got;
+}
+
+}  // namespace kgio

@@ -1,0 +1,71 @@
+// kgwas_io.hpp -- file readers of the kgwas program.
+//
+// Same inputs, checks and [ERROR] messages as the reference's readers
+// (src/kgwas_utils.hpp), but the column matrix is packed straight into
+// k-mer-major bit rows (1 bit per sample) instead of an n x N float matrix.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+namespace kgio {
+
+[[noreturn]] void die(const std::string& m);   // "[ERROR] m", exit(1)
+void warn(const std::string& m);               // "[WARN] m"
+int env_int(const char* k, int dflt);          // src/kgwas_utils.hpp:43-47
+
+struct Timer {
+  double t0;
+  Timer();
+  double sec() const;
+};
+
+// src/kgwas_utils.hpp:51-61: skip empty lines, drop one trailing '\r'.
+std::vector<std::string> load_lines(const std::string& file);
+// src/kgwas_utils.hpp:63-70: whitespace-separated "id value"; last duplicate wins.
+std::unordered_map<std::string, double> load_pheno(const std::string& file);
+
+struct Overlap {                                // src/kgwas_utils.hpp:285-314
+  std::vector<int> idxs;                        // positions in samples.txt
+  std::vector<std::string> samples;
+  std::vector<double> y;
+};
+Overlap build_overlap(const std::string& samples_file, const std::string& pheno_file);
+
+struct UData {                                  // src/kgwas_utils.hpp:129-157
+  std::vector<double> U;                        // n x k column-major
+  int n = 0, k = 0;
+};
+UData load_ubin(const std::string& path, int n);
+
+size_t infer_N_from_bits(const std::string& bits_dir, int first_idx);   // :317-332
+std::vector<std::string> load_kmers(const std::string& path, size_t N);  // :93-127
+
+inline uint32_t words_per_kmer(int n) {
+  uint32_t w = (uint32_t)((n + 63) / 64);
+  return w + (w & 1u);
+}
+
+// src/kgwas_utils.hpp:225-282: column k of the overlap is bits/col_%06d of
+// idxs[k] (.txt preferred over .txt.gz); row i is byte i & 1.  Writes
+// N x words_per_kmer(n) packed words into `out` (caller-allocated).
+void load_matrix_packed(const std::string& bits_dir, const std::vector<int>& idxs, size_t N, int threads,
+                        uint64_t* out);
+
+// ROWS-mode input (src/kgwas.cpp:435-459): "kmer<TAB or SPACE>bitstring" lines,
+// x_j = (bits[idxs[j]] == '1').  Appends to kmers/packed.
+struct RowsReader {
+  explicit RowsReader(const std::string& path);
+  ~RowsReader();
+  // Reads up to max_rows rows; returns the number read (0 at end).
+  size_t read(size_t max_rows, const std::vector<int>& idxs, std::vector<std::string>& kmers,
+              std::vector<uint64_t>& packed);
+  size_t lines = 0;   // non-empty lines seen (the reference's line_count)
+ private:
+  void* gz = nullptr;
+  void* plain = nullptr;
+  bool next_line(std::string& line);
+};
+
+}  // namespace kgio

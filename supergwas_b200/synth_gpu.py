@@ -1,0 +1,70 @@
+"""Device-side generator of large seeded synthetic batches (bench workloads).
+
+Same Balding-Nichols model as :mod:`supergwas_b200.synth` (ancestral
+p ~ Beta(0.5, 0.5), per-subpopulation p_s ~ Beta(p(1-F)/F, (1-p)(1-F)/F),
+F = 0.1, x ~ Bernoulli(p_s)), written straight into the packed k-mer-major
+layout in device memory, chunk by chunk, each chunk from its own seeded
+generator.  The structure matrix U and the phenotype y are then built on the
+host from a 50,000-k-mer sample and the causal k-mers, exactly as in
+:func:`supergwas_b200.synth.simulate`.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import synth
+
+
+def gen_packed(n: int, m: int, S: int, seed: int, device: str = "cuda", chunk: int = 1 << 20,
+               out: torch.Tensor | None = None) -> torch.Tensor:
+    """(m, words_per_kmer(n)) int64 tensor of packed rows on `device`."""
+    W = synth.words_per_kmer(n)
+    if out is None:
+        out = torch.empty((m, W), dtype=torch.int64, device=device)
+    pop = torch.as_tensor((np.arange(n) * S) // n, device=device)
+    weights = (2 ** torch.arange(8, device=device, dtype=torch.int32)).to(torch.uint8)
+    c = (1.0 - synth.F_ST) / synth.F_ST
+    for s in range(0, m, chunk):
+        e = min(m, s + chunk)
+        cm = e - s
+        g = torch.Generator(device=device)
+        g.manual_seed(int(seed) * 1_000_003 + s // chunk)
+        u = torch.rand(cm, generator=g, device=device, dtype=torch.float64)
+        p = torch.sin(0.5 * torch.pi * u) ** 2            # Beta(0.5, 0.5) (arcsine law)
+        p = p.clamp(1e-6, 1 - 1e-6)
+        a = (p * c).unsqueeze(1).expand(cm, S)
+        b = ((1 - p) * c).unsqueeze(1).expand(cm, S)
+        ga = torch._standard_gamma(a.contiguous())
+        gb = torch._standard_gamma(b.contiguous())
+        ps = torch.nan_to_num(ga / (ga + gb), nan=0.5).to(torch.float32)
+        probs = ps[:, pop]                                   # (cm, n)
+        bits = torch.rand(cm, n, generator=g, device=device, dtype=torch.float32) < probs
+        del probs
+        if W * 64 > n:
+            bits = torch.cat([bits, torch.zeros(cm, W * 64 - n, dtype=torch.bool, device=device)], 1)
+        by = (bits.view(cm, W * 8, 8).to(torch.uint8) * weights).sum(-1, dtype=torch.int32).to(torch.uint8)
+        out[s:e] = by.view(torch.int64).view(cm, W)
+        del bits, by
+    return out
+
+
+def structure_and_phenotype(packed_dev: torch.Tensor, n: int, r: int, n_causal: int, missing: float,
+                            seed: int, structure_kmers: int = 50_000):
+    """U (overlap x (r+1)), y and overlap indices for a device-resident batch."""
+    rng = np.random.default_rng(seed)
+    m = packed_dev.shape[0]
+    n_miss = int(round(missing * n))
+    miss = np.sort(rng.choice(n, size=n_miss, replace=False)) if n_miss else np.zeros(0, np.int64)
+    keep = np.setdiff1d(np.arange(n), miss)
+    sk = min(structure_kmers, m)
+    sidx = np.sort(rng.choice(m, size=sk, replace=False))
+    rows = packed_dev[torch.as_tensor(sidx, device=packed_dev.device)].cpu().numpy().view(np.uint64)
+    Xs = synth.unpack_rows(rows, n)[:, keep].T
+    U, Ph = synth.structure_basis(Xs, r)
+    causal = np.sort(rng.choice(m, size=n_causal, replace=False))
+    beta = rng.standard_normal(n_causal)
+    crow = packed_dev[torch.as_tensor(causal, device=packed_dev.device)].cpu().numpy().view(np.uint64)
+    g = beta @ synth.unpack_rows(crow, n)[:, keep].astype(np.float64)
+    y = g + 0.5 * Ph[:, -1] + rng.standard_normal(keep.shape[0])
+    return U, y, keep, causal

@@ -1,0 +1,75 @@
+"""The kgwas program against the reference's own output files.
+
+Integer parity (row set, row order, k-mer strings, .2d bitstrings, .count)
+is exact outside the tolerance band of the pre-filter and emit cuts; floats
+agree to the reference's print precision (ROWS mode, FP64) or its FP32
+resolution (COLS mode).
+"""
+import os
+import tempfile
+
+import pytest
+
+import helpers as H
+from oracle import oracle as O
+from test_oracle_golden import COLS_REL, ROWS_REL, _log10, _thr
+
+pytestmark = pytest.mark.gpu
+
+
+def _check_outputs(out, name, mode, variant, kmers, band):
+    tol = ROWS_REL if mode == "rows" else COLS_REL
+    got = open(out + ".count").read()
+    ref = open(H.ref_file(name, mode, variant["name"], ".tsv.count")).read()
+    if band:
+        assert abs(int(got.split("\t")[1]) - int(ref.split("\t")[1])) <= len(band)
+        assert got.split("\t")[0] == ref.split("\t")[0]
+    else:
+        assert got == ref
+    H.compare_rows(H.parse_rows(out), H.parse_rows(H.ref_file(name, mode, variant["name"], ".tsv")),
+                   kmers, band, tol)
+    ref2 = H.parse_rows(H.ref_file(name, mode, variant["name"], ".2d.tsv"))
+    got2 = H.parse_rows(O.path_2d(out))
+    assert (ref2 is None) == (got2 is None)
+    if ref2 is not None:
+        H.compare_rows(got2, ref2, kmers, band, tol)
+
+
+@pytest.mark.parametrize("prec", ["split", "fp64"])
+@pytest.mark.parametrize("name", H.FIXTURES)
+def test_cli_matches_reference(built, name, prec):
+    fx = H.load_fixture(name)
+    n = int(fx["idxs"].shape[0])
+    work = tempfile.mkdtemp()
+    paths, rows = H.materialise(name, work)
+    for v in H.meta(name)["variants"]:
+        st = O.cols_stats(fx["packed"], n, fx["U"], fx["y"], _thr(v))
+        band = H.band_kmers(st, _thr(v), _log10(v))
+        for mode, inp in (("cols", paths["batch"]), ("rows", rows)):
+            out = os.path.join(work, f"{mode}_{v['name']}", "batch_000.tsv")
+            os.makedirs(os.path.dirname(out))
+            env = dict(v.get("env", {}))
+            env["KGWAS_PRECISION"] = prec
+            r = H.run_cli([paths["samples"], paths["pheno"], inp, paths["ubin"], out, *v["args"],
+                           "--mode", mode], env)
+            assert r.returncode == 0, r.stderr[-2000:]
+            _check_outputs(out, name, mode, v, fx["kmers"], band)
+
+
+@pytest.mark.slow
+def test_cli_matches_reference_cfg1(built):
+    """Config 1: n=200 (190 phenotyped), m=1e6, r=5+1, auto-detected COLS mode and gz ROWS input."""
+    ds = H.load_cfg1()
+    X = ds.packed_overlap()
+    work = tempfile.mkdtemp()
+    paths, rows = H.materialise_cfg1(work)
+    for v in H.meta("cfg1")["variants"]:
+        st = O.cols_stats(X, ds.n, ds.U, ds.y, _thr(v))
+        band = H.band_kmers(st, _thr(v), _log10(v))
+        for mode, inp in (("cols", paths["batch"]), ("rows", rows)):
+            out = os.path.join(work, f"{mode}_{v['name']}", "batch_000.tsv")
+            os.makedirs(os.path.dirname(out))
+            r = H.run_cli([paths["samples"], paths["pheno"], inp, paths["ubin"], out, *v["args"]],
+                          v.get("env", {}))
+            assert r.returncode == 0, r.stderr[-2000:]
+            _check_outputs(out, "cfg1", mode, v, ds.kmers, band)

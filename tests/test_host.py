@@ -1,0 +1,169 @@
+"""CPU-only checks: the C ABI library, host-side algebra, formats and CLI errors."""
+import ctypes
+import json
+import os
+import shutil
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import helpers as H
+from oracle import oracle as O
+from supergwas_b200 import api, build, synth
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def test_library_exports_every_header_symbol(built):
+    L = api.lib()
+    syms = api.header_symbols()
+    assert len(syms) >= 12
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+    assert api.version().startswith("kgwas-b200")
+
+
+def test_default_opts_match_reference_defaults(built):
+    o = api._Opts()
+    api.lib().kg_default_opts(ctypes.byref(o))
+    assert o.corr_threshold == 0.2        # src/kgwas.cpp:30
+    assert o.log10_thresh == 6.0          # src/kgwas.cpp:28
+    assert o.precision == api.PREC["split"]
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-GPU error path")
+def test_create_without_gpu_fails_cleanly(built):
+    with pytest.raises(api.KgError) as e:
+        api.Kgwas()
+    assert e.value.code in (2, 6)
+
+
+def test_pack_roundtrip():
+    rng = np.random.default_rng(0)
+    for n in (1, 63, 64, 65, 200, 1000):
+        x = (rng.random((37, n)) < 0.4).astype(np.uint8)
+        p = synth.pack_rows(x)
+        assert p.shape[1] == synth.words_per_kmer(n) and p.shape[1] % 2 == 0
+        assert np.array_equal(synth.unpack_rows(p, n), x)
+
+
+def test_ubin_roundtrip(tmp_path):
+    U = np.random.default_rng(1).standard_normal((17, 4))
+    synth.write_ubin(tmp_path / "U.bin", U)
+    b = (tmp_path / "U.bin").read_bytes()
+    assert np.frombuffer(b[:8], np.int32).tolist() == [17, 4]
+    assert np.array_equal(synth.read_ubin(tmp_path / "U.bin"), U)
+
+
+def test_count_and_2d_names():
+    assert O.count_line("/a/b/batch_000.tsv", 7) == "batch_000\t7\n"
+    assert O.count_line("x.y.tsv", 1) == "x.y\t1\n"
+    assert O.path_2d("/a/b.tsv") == "/a/b.2d.tsv"
+    assert O.path_2d("noext") == "noext.2d"
+
+
+# ---------------------------------------------------- host algebra on the CPU
+
+_EMU = None
+
+
+def emu_lib():
+    global _EMU
+    if _EMU is None:
+        out = os.path.join(HERE, "native", "_build", "libprep_check.so")
+        src = [os.path.join(HERE, "native", "prep_check.cpp"),
+               os.path.join(build.CSRC, "prep.cpp")]
+        if not os.path.exists(out) or any(os.path.getmtime(s) > os.path.getmtime(out) for s in src):
+            os.makedirs(os.path.dirname(out), exist_ok=True)
+            subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-o", out, *src], check=True)
+        _EMU = ctypes.CDLL(out)
+    return _EMU
+
+
+def emulate(packed, n, U, y, split, lu=3, ly=5, thr=0.0):
+    L = emu_lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    packed = np.ascontiguousarray(packed)
+    m, wpk = packed.shape
+    Uc = np.ascontiguousarray(np.asarray(U).T)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    f = ("chisq", "effect", "xxM", "xyM", "cor")
+    out = {k: np.zeros(m) for k in f}
+    t = np.zeros(m, np.uint8)
+    yy = ctypes.c_double()
+    rc = L.prep_emulate(Uc.ctypes.data_as(dp), n, U.shape[1], y.ctypes.data_as(dp),
+                        packed.ctypes.data_as(ctypes.c_void_p), ctypes.c_int64(m), wpk, split, lu, ly,
+                        ctypes.c_double(thr), t.ctypes.data_as(ctypes.c_void_p),
+                        *[out[k].ctypes.data_as(dp) for k in f], ctypes.byref(yy))
+    assert rc == 0
+    out["tested"] = t.astype(bool)
+    return out
+
+
+@pytest.mark.parametrize("split", [0, 1])
+def test_prep_algebra_matches_oracle(split):
+    """prepare()/make_limbs() + the kernels' arithmetic, replayed on the CPU."""
+    for (n, m, S, r, seed) in [(200, 20000, 5, 5, 1), (1000, 8000, 8, 16, 2), (61, 3000, 3, 3, 3)]:
+        ds = synth.simulate(n=n, m=m, S=S, r=r, n_causal=20, missing=0.05, seed=seed)
+        X = ds.packed_overlap()
+        o = O.cols_stats(X, ds.n, ds.U, ds.y, 0.0)
+        e = emulate(X, ds.n, ds.U, ds.y, split)
+        assert np.array_equal(e["tested"], o["tested"])
+        msk = o["tested"]
+        rel = np.abs(e["chisq"] - o["chisq"]) / np.maximum(o["chisq"], 1e-300)
+        ml = np.abs(O.mlog10p(e["chisq"]) - o["mlog10p"])
+        if split:
+            assert np.percentile(rel[msk], 99) <= 1e-6
+            assert ml[msk].max() <= 1e-6
+        else:
+            assert rel[msk].max() <= 1e-9
+            assert ml[msk].max() <= 1e-11
+
+
+def test_prep_general_U_without_intercept():
+    """U that does not contain the constant vector (no intercept column)."""
+    fx = H.load_fixture("edge")
+    n = int(fx["idxs"].shape[0])
+    o = O.cols_stats(fx["packed"], n, fx["U"], fx["y"], 0.0)
+    for split in (0, 1):
+        e = emulate(fx["packed"], n, fx["U"], fx["y"], split)
+        assert np.array_equal(e["tested"], o["tested"])
+        ml = np.abs(O.mlog10p(e["chisq"]) - o["mlog10p"])
+        assert ml[o["tested"]].max() <= 1e-6
+
+
+# ---------------------------------------------------------- CLI error paths
+
+def _fault_cases():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(H.GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg
+
+
+def test_cli_errors_match_reference(built):
+    """Malformed inputs give the reference's [ERROR] line and exit code 1,
+    before any GPU work (src/kgwas_utils.hpp:34-37)."""
+    mg = _fault_cases()
+    expected = json.load(open(os.path.join(H.GOLDEN, "faults.json")))
+    for name, mutate, env in mg.fault_cases():
+        work, w = mg.fault_workdir()
+        try:
+            argv = mutate(w)
+            r = H.run_cli(argv, env)
+            exp = expected[name]
+            assert r.returncode == exp["rc"], (name, r.returncode, r.stderr[-500:])
+            assert mg.error_line(r.stderr, work) == exp["error"], (name, r.stderr[-500:])
+        finally:
+            shutil.rmtree(work)
