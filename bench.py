@@ -388,7 +388,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--kmers", type=int, default=0, help="k-mers per GPU (default 2e8)")
-    ap.add_argument("--e2e-kmers", type=int, default=0, help="k-mers of the end-to-end leg (default all)")
+    ap.add_argument("--e2e-kmers", type=int, default=50_000_000,
+                    help="k-mers per step of the end-to-end leg (pinned host batch; 0 = all)")
     ap.add_argument("--acc-kmers", type=int, default=200_000)
     ap.add_argument("--cpu-kmers", type=int, default=1_000_000)
     ap.add_argument("--ref-kmers", type=int, default=250_000)

@@ -5,7 +5,8 @@ reference kgwas binary (COLS mode, FP32 linear algebra, src/kgwas.cpp:138-166;
 ROWS mode, FP64, src/kgwas.cpp:455-476).  The oracle must reproduce:
   * the .count value and the emitted k-mer rows, in order, exactly, except for
     k-mers inside the tolerance band of the pre-filter or emit cut;
-  * ROWS-mode floats to the reference's 6-significant-digit print precision;
+  * ROWS-mode floats to the reference's 6-significant-digit print precision
+    (values at a rounding boundary may differ by one unit in the last digit);
   * COLS-mode floats to the reference's FP32 resolution.
 """
 import os
@@ -16,7 +17,7 @@ import pytest
 import helpers as H
 from oracle import oracle as O
 
-ROWS_REL = 6e-6      # 6 printed significant digits (half-ulp 5e-6) + rounding
+ROWS_REL = 1.1e-5    # 6 printed significant digits: one unit in the last digit is <= 1e-5 relative
 COLS_REL = 2e-2      # reference COLS computes xxM/xyM in FP32 (measured <= 6.5e-3)
 
 
