@@ -141,6 +141,11 @@ void kg_host_free(void* p);
 /* Number of kernel launches the last kg_run_host / kg_launch_device made. */
 int kg_last_launch_count(const kg_ctx* ctx);
 
+/* Which association kernel the last launch used: "ts" (tensor cores, x
+ * unpacked into tensor memory), "ss" (tensor cores, x unpacked into shared
+ * memory; shapes the first does not cover) or "fp64" (CUDA cores). */
+const char* kg_last_kernel(const kg_ctx* ctx);
+
 const char* kg_last_error(const kg_ctx* ctx);
 void kg_destroy(kg_ctx* ctx);
 

@@ -87,6 +87,8 @@ def lib():
     L.kg_launch_device_stats.argtypes = [vp, vp, ctypes.c_uint64, ctypes.c_uint32, vp]
     L.kg_fetch.argtypes = [vp, ctypes.POINTER(_Result), ctypes.POINTER(_Stats)]
     L.kg_last_launch_count.argtypes = [vp]
+    L.kg_last_kernel.argtypes = [vp]
+    L.kg_last_kernel.restype = ctypes.c_char_p
     L.kg_last_error.argtypes = [vp]
     L.kg_last_error.restype = ctypes.c_char_p
     L.kg_destroy.argtypes = [vp]
@@ -226,6 +228,9 @@ class Kgwas:
 
     def last_launch_count(self) -> int:
         return int(self._L.kg_last_launch_count(self._h))
+
+    def last_kernel(self) -> str:
+        return self._L.kg_last_kernel(self._h).decode()
 
 
 def version() -> str:

@@ -19,6 +19,24 @@ namespace {
 
 constexpr int NBUF = 2;  // host-run chunk buffers in flight
 
+// Smallest r2 that can still give p = erfc(sqrt(T/2)) <= p_thresh with
+// T = n log(1/(1-r2)) (src/kgwas.cpp:51-52), lowered by a relative margin of
+// 1e-9 so that k-mers below it are certainly not emitted.  -1 when every
+// tested k-mer may be emitted.
+double r2_candidate(double p_thresh, int n) {
+  if (!(p_thresh < 1.0)) return -1.0;
+  if (p_thresh <= 0.0) return 2.0;
+  double lo = 0.0, hi = 1.0;
+  while (std::erfc(std::sqrt(0.5 * hi)) > p_thresh && hi < 1e7) hi *= 2;
+  for (int it = 0; it < 200; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (std::erfc(std::sqrt(0.5 * mid)) > p_thresh) lo = mid; else hi = mid;
+  }
+  const double T = lo;  // erfc(sqrt(T/2)) > p_thresh for every T < lo
+  const double r2 = -std::expm1(-T / (double)n);
+  return r2 * (1.0 - 1e-9);
+}
+
 template <class T>
 void dfree(T*& p) {
   if (p) cudaFree((void*)p);
@@ -41,7 +59,8 @@ struct kg_ctx {
   // structure on the device
   double* dV = nullptr;
   int cm = 0, nsteps = 0;
-  int8_t* dB = nullptr;
+  int8_t* dB = nullptr;      // B image of the smem-A kernel
+  int8_t* dBts = nullptr;    // B image of the TMEM-A kernel
   int nchunk = 0;
   // outputs on the device
   unsigned long long* dCounters = nullptr;
@@ -61,6 +80,7 @@ struct kg_ctx {
   bool pend_stats = false;
   cudaStream_t pend_stream = nullptr;
   int launches = 0;
+  const char* last_kernel = "";
   // host-run buffers
   uint64_t* dChunk[NBUF] = {};
   void* hStage[NBUF] = {};
@@ -151,6 +171,7 @@ void kg_destroy(kg_ctx* ctx) {
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   dfree(ctx->dV);
   dfree(ctx->dB);
+  dfree(ctx->dBts);
   dfree(ctx->dCounters);
   dfree(ctx->dHits);
   dfree(ctx->dTested);
@@ -169,6 +190,8 @@ void kg_destroy(kg_ctx* ctx) {
 const char* kg_last_error(const kg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 int kg_last_launch_count(const kg_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+const char* kg_last_kernel(const kg_ctx* ctx) { return ctx ? ctx->last_kernel : ""; }
 
 int kg_set_structure_ex(kg_ctx* ctx, const double* U, int n, int k, const double* y, const int32_t* sample_pos,
                         int n_row_samples, double* yyM_out) {
@@ -198,6 +221,7 @@ int kg_set_structure_ex(kg_ctx* ctx, const double* U, int n, int k, const double
   P.ynorm = p.ynorm;
   P.corr_thr = ctx->opts.corr_threshold;
   P.p_thresh = std::pow(10.0, -ctx->opts.log10_thresh);
+  P.r2_cand = r2_candidate(P.p_thresh, n);
   for (int j = 0; j < k; ++j) {
     P.a[j] = p.a[j];
     P.g[j] = p.g[j];
@@ -240,6 +264,10 @@ int kg_set_structure_ex(kg_ctx* ctx, const double* U, int n, int k, const double
     dfree(ctx->dB);
     KG_CUDA(cudaMalloc((void**)&ctx->dB, img.size()), "cudaMalloc(B)");
     KG_CUDA(cudaMemcpy(ctx->dB, img.data(), img.size(), cudaMemcpyHostToDevice), "copy B");
+    kg::make_b_image_ts(ctx->limbs, img);
+    dfree(ctx->dBts);
+    KG_CUDA(cudaMalloc((void**)&ctx->dBts, img.size()), "cudaMalloc(B)");
+    KG_CUDA(cudaMemcpy(ctx->dBts, img.data(), img.size(), cudaMemcpyHostToDevice), "copy B");
   }
   ctx->have_structure = true;
   return KG_OK;
@@ -304,9 +332,25 @@ int launch_one(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, uint64
   if (ctx->opts.precision == KG_PREC_FP64) {
     kg::LaunchFp64 L{dx, m, (int)wpk, ctx->dV, ctx->nsteps, ctx->cm, &ctx->P, &O, ctx->num_sms};
     e = kg::launch_fp64(L, st);
+    ctx->last_kernel = "fp64";
   } else {
-    kg::LaunchTc L{dx, m, (int)wpk, ctx->nchunk, ctx->dB, &ctx->P, &ctx->LM, &O, ctx->num_sms};
-    e = kg::launch_tc(L, st);
+    const char* force = std::getenv("KG_KERNEL");
+    const bool want_ss = force && std::string(force) == "ss";
+    const bool ts_ok = kg::ts_supported(ctx->limbs.N, ctx->opts.limbs_u, ctx->opts.limbs_y, ctx->limbs.Kpad,
+                                        (int)wpk) &&
+                       ((uintptr_t)dx % 16) == 0;
+    if (force && std::string(force) == "ts" && !ts_ok)
+      return ctx->fail(KG_ERR_UNSUPPORTED, "KG_KERNEL=ts: shape not supported by the TMEM-A kernel");
+    if (ts_ok && !want_ss) {
+      kg::LaunchTs L{dx, m, (int)wpk, ctx->limbs.Kpad, ctx->prep.drop0 && ctx->P.k > 0, ctx->dBts, &ctx->P,
+                     &ctx->LM, &O, ctx->num_sms};
+      e = kg::launch_ts(L, st);
+      ctx->last_kernel = "ts";
+    } else {
+      kg::LaunchTc L{dx, m, (int)wpk, ctx->nchunk, ctx->dB, &ctx->P, &ctx->LM, &O, ctx->num_sms};
+      e = kg::launch_tc(L, st);
+      ctx->last_kernel = "ss";
+    }
   }
   if (e != cudaSuccess) return ctx->cuda_fail(e, "kernel launch");
   ++ctx->launches;

@@ -170,9 +170,13 @@ __device__ __forceinline__ void finish_kmer(const EpiParams& P, const DevOut& O,
       double r2 = (xyM * xyM) / (xxM * P.yyM);
       if (r2 < 0) r2 = 0;
       if (r2 >= 1) r2 = 1 - 1e-15;
-      T = (double)n * log(1.0 / (1.0 - r2));
-      p = erfc(sqrt(0.5 * T));
-      effect = xyM / (xxM * P.yyM);
+      if (O.tested || r2 >= P.r2_cand) {
+        T = (double)n * log(1.0 / (1.0 - r2));
+        p = erfc(sqrt(0.5 * T));
+        effect = xyM / (xxM * P.yyM);
+      } else {
+        p = 2.0;  // provably above p_thresh; the row is not emitted and no stats are kept
+      }
     }
   }
   const bool hit = tested && p <= P.p_thresh;

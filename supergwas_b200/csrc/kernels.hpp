@@ -33,6 +33,23 @@ int fp64_cm(int C);           // padded column count for C contraction columns (
 int fp64_steps(int n);        // 128-sample steps covering n samples
 cudaError_t launch_fp64(const LaunchFp64& L, cudaStream_t st);
 
+struct LaunchTs {
+  const uint64_t* x;          // packed rows (device), 16-byte aligned
+  unsigned long long m;
+  int wpk;
+  int kpad;                   // samples covered by the B image (multiple of 128)
+  bool drop0;                 // U column 0 has no limbs (intercept handled in FP64)
+  const int8_t* Bimg;         // make_b_image_ts layout (device)
+  const EpiParams* P;
+  const LimbMap* LM;
+  const DevOut* O;
+  int num_sms;
+};
+
+// TMEM-A kernel: 3 limbs per U column, 5 for y', N <= 128, B resident in smem.
+bool ts_supported(int N, int limbs_u, int limbs_y, int kpad, int wpk);
+cudaError_t launch_ts(const LaunchTs& L, cudaStream_t st);
+
 int tc_kc();                  // samples per K chunk of the tensor-core kernel
 bool tc_supported_n(int N);
 cudaError_t launch_tc(const LaunchTc& L, cudaStream_t st);

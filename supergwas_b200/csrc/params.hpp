@@ -11,6 +11,7 @@ namespace kg {
 struct EpiParams {
   int n, k;
   double b, kappa, yyM, ynorm, corr_thr, p_thresh;
+  double r2_cand;   // r2 below this cannot give p <= p_thresh (log/erfc skipped)
   double a[KMAX];
   double g[KMAX];
 };

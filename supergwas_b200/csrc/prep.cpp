@@ -129,11 +129,16 @@ std::string make_limbs(const Prepared& p, const int* pos, int n_row, int limbs_u
   if (n_row < n) return "rows hold fewer samples than the overlap";
   L = LimbCols();
   L.Kpad = ((n_row + kquant - 1) / kquant) * kquant;
+  // column order: [count, y' limbs, U column 0 (unless dropped), U columns 1..k-1]
   int col = 0;
   L.count_col = col++;
-  for (int j = 0; j <= k; ++j) {
-    const bool skip = (j == 0 && k > 0 && p.drop0);
-    const int nl = skip ? 0 : (j == k ? limbs_y : limbs_u);
+  L.first[k] = col;
+  L.nl[k] = limbs_y;
+  L.scale[k] = 0.0;
+  col += limbs_y;
+  for (int j = 0; j < k; ++j) {
+    const bool skip = (j == 0 && p.drop0);
+    const int nl = skip ? 0 : limbs_u;
     L.first[j] = col;
     L.nl[j] = nl;
     L.scale[j] = 0.0;
@@ -170,6 +175,21 @@ std::string make_limbs(const Prepared& p, const int* pos, int n_row, int limbs_u
     }
   }
   return "";
+}
+
+void make_b_image_ts(const LimbCols& L, std::vector<int8_t>& img) {
+  const int N = L.N;
+  img.assign((size_t)L.Kpad * N, 0);
+  for (int kap = 0; kap < L.Kpad; ++kap) {
+    // TMEM column c of a 128-sample stage holds K = 4c..4c+3; byte t of column
+    // 8q+j is sample 32q + 8t + j of the stage (see the unpack in kernel_ts.cu)
+    const int a = kap / 128, w = kap % 128, c = w / 4, t = w % 4, q = c / 8, j = c % 8;
+    const int i = 128 * a + 32 * q + 8 * t + j;
+    for (int col = 0; col < N; ++col) {
+      const size_t off = (size_t)(kap / 16) * (N * 16) + (size_t)(col / 8) * 128 + (size_t)(col % 8) * 16 + kap % 16;
+      img[off] = L.vals[(size_t)col * L.Kpad + i];
+    }
+  }
 }
 
 void make_b_image(const LimbCols& L, int KC, std::vector<int8_t>& img) {

@@ -41,7 +41,9 @@ struct Prepared {
 // Returns an empty string on success, else the error text.
 std::string prepare(const double* U_colmajor, int n, int k, const double* y, Prepared& out);
 
-// int8 limb form of the contraction columns for tcgen05 kind::i8.
+// int8 limb form of the contraction columns for tcgen05 kind::i8.  Column
+// order: count (1 for every phenotyped sample), the y' limbs, then the limbs
+// of U columns 0 (unless drop0) .. k-1.
 struct LimbCols {
   int N = 0;                    // MMA N (columns incl. padding), multiple of 16
   int count_col = 0;            // column holding 1 for every sample (popcount)
@@ -65,5 +67,11 @@ std::string make_limbs(const Prepared& p, const int* pos, int n_row, int limbs_u
 // another (UMMA K-major, no swizzle: 8-row x 16-byte core matrices, core
 // (n8, k16) of chunk q at q*KC*N + k16*(N*16) + n8*128).
 void make_b_image(const LimbCols& L, int KC, std::vector<int8_t>& img);
+
+// B operand image for the TMEM-A kernel: the whole Kpad x N matrix in one
+// K-major no-swizzle layout (core (n8, k16) at k16*(N*16) + n8*128), with the
+// K index permuted inside every 128-sample stage to match the bit unpack
+// order: K = 4c + t of column c = 8q + j holds sample 32q + 8t + j.
+void make_b_image_ts(const LimbCols& L, std::vector<int8_t>& img);
 
 }  // namespace kg

@@ -87,6 +87,9 @@ def structure_basis(Xs: np.ndarray, r: int) -> np.ndarray:
     (sample sd, n-1), prepend a column of ones and take the thin SVD's U.
     """
     X = Xs.astype(np.float64)
+    n = X.shape[0]
+    if r <= 0 or n < 2:
+        return np.full((n, 1), 1.0 / np.sqrt(n)), np.zeros((n, 0))
     X = X - X.mean(axis=0, keepdims=True)
     G = X @ X.T
     evals, evecs = np.linalg.eigh(G)
@@ -164,7 +167,8 @@ def simulate(n: int, m: int, S: int, r: int, n_causal: int, missing: float,
     if n_causal:
         Xc = unpack_rows(packed[causal], n)[:, keep].astype(np.float64)
         g = beta @ Xc
-    y = g + 0.5 * Ph[:, -1] + rng.standard_normal(keep.shape[0])
+    pc1 = Ph[:, -1] if Ph.shape[1] else 0.0
+    y = g + 0.5 * pc1 + rng.standard_normal(keep.shape[0])
     kmers = random_kmers(rng, m, kmer_len)
     return Dataset(n_all=n, samples=samples, pheno_ids=[samples[i] for i in keep],
                    y=y, idxs=keep.astype(np.int64), U=U, packed_all=packed,

@@ -66,5 +66,6 @@ def structure_and_phenotype(packed_dev: torch.Tensor, n: int, r: int, n_causal: 
     beta = rng.standard_normal(n_causal)
     crow = packed_dev[torch.as_tensor(causal, device=packed_dev.device)].cpu().numpy().view(np.uint64)
     g = beta @ synth.unpack_rows(crow, n)[:, keep].astype(np.float64)
-    y = g + 0.5 * Ph[:, -1] + rng.standard_normal(keep.shape[0])
+    pc1 = Ph[:, -1] if Ph.shape[1] else 0.0
+    y = g + 0.5 * pc1 + rng.standard_normal(keep.shape[0])
     return U, y, keep, causal
