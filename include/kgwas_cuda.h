@@ -152,6 +152,36 @@ void kg_destroy(kg_ctx* ctx);
 /* Library version string. */
 const char* kg_version(void);
 
+/* Allocation-free run, for callers that may not allocate device memory (a
+ * host framework that owns every device byte through its own pool, a plugin
+ * inside such a process, a job with a fixed memory budget).  No counterpart
+ * in the reference.
+ *
+ * Runs the split-precision test of kg_set_structure + kg_launch_device in one
+ * call, without a context: d_xbits (device, packed rows as above), U/y (host,
+ * as in kg_set_structure), and d_hits (device, hit_capacity records, filled
+ * in arbitrary order).  counts_out (host) receives {n_tested, n_hits}.  The
+ * call is synchronous on `stream` (a cudaStream_t, NULL = default stream).
+ *
+ * It calls no device allocator.  Its device scratch (the int8 limb image of
+ * the structure and the counters) is one static array of
+ * KG_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds until
+ * the process exits; structures whose image exceeds KG_NOALLOC_MAX_B_BYTES
+ * (overlap samples rounded up to 256, times the limb columns rounded up to 16)
+ * are rejected with KG_ERR_UNSUPPORTED.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) and should come before
+ * any stream capture on that device.  Calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller.  More hits
+ * than hit_capacity return KG_ERR_INVALID with counts_out still filled.
+ * err (optional, err_len bytes) receives a message on failure. */
+#define KG_NOALLOC_MAX_B_BYTES (256u * 1024u)
+#define KG_NOALLOC_SCRATCH_BYTES (KG_NOALLOC_MAX_B_BYTES + 256u)
+int kg_run_device_noalloc(const uint64_t* d_xbits, uint64_t n_kmers, uint32_t words_per_kmer,
+                          const double* U_colmajor, int n, int k, const double* y,
+                          double corr_threshold, double log10_thresh,
+                          kg_hit* d_hits, uint64_t hit_capacity, uint64_t* counts_out,
+                          void* stream, char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -98,6 +98,9 @@ def lib():
     L.kg_host_alloc.restype = vp
     L.kg_host_free.argtypes = [vp]
     L.kg_host_free.restype = None
+    L.kg_run_device_noalloc.argtypes = [vp, ctypes.c_uint64, ctypes.c_uint32, _DP, ctypes.c_int, ctypes.c_int,
+                                        _DP, ctypes.c_double, ctypes.c_double, vp, ctypes.c_uint64,
+                                        ctypes.POINTER(ctypes.c_uint64), vp, ctypes.c_char_p, ctypes.c_size_t]
     _LIB = L
     return L
 
@@ -231,6 +234,25 @@ class Kgwas:
 
     def last_kernel(self) -> str:
         return self._L.kg_last_kernel(self._h).decode()
+
+
+def run_device_noalloc(d_x: int, m: int, wpk: int, U, y, corr_threshold: float, log10_thresh: float,
+                       d_hits: int, hit_capacity: int, stream: int | None = None):
+    """Call kg_run_device_noalloc: no context, no device allocation.
+
+    For callers that may not allocate device memory themselves: rows (d_x)
+    and the hit buffer (d_hits, hit_capacity records of HIT_DTYPE) are device
+    pointers the caller owns.  Returns (rc, n_tested, n_hits, message)."""
+    U = np.asarray(U, dtype=np.float64)
+    n, k = U.shape
+    Uc = np.ascontiguousarray(U.T)
+    yv = np.ascontiguousarray(y, dtype=np.float64)
+    counts = (ctypes.c_uint64 * 2)()
+    msg = ctypes.create_string_buffer(512)
+    rc = lib().kg_run_device_noalloc(d_x, m, wpk, Uc.ctypes.data_as(_DP), n, k, yv.ctypes.data_as(_DP),
+                                     corr_threshold, log10_thresh, d_hits, hit_capacity, counts, stream,
+                                     msg, len(msg))
+    return rc, int(counts[0]), int(counts[1]), msg.value.decode()
 
 
 def version() -> str:

@@ -1,0 +1,85 @@
+"""The allocation-free entry point, kg_run_device_noalloc.
+
+It exists for callers that may not allocate device memory -- a framework
+that owns every device byte through its own pool, a plugin inside such a
+process, a job whose memory budget is fixed before it runs.  They pass their
+own device buffers for the packed rows and for the emitted rows; the call's
+only other device memory is a fixed static array inside the library.
+
+These tests call it through the C ABI and check it against the existing
+entry point (kg_set_structure + kg_run_host) on two calls in a row -- the
+second with another phenotype, thresholds and batch, so a stale counter or
+limb image left by the first call would show -- and check the size limit and
+the short-buffer report.  This file is collected last on purpose.
+"""
+import numpy as np
+import pytest
+
+from supergwas_b200 import api, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _device_call(X, U, y, thr, lt, cap):
+    import torch
+    dx = torch.from_numpy(np.ascontiguousarray(X).view(np.int64)).cuda()
+    hits = torch.zeros((max(cap, 1), 4), dtype=torch.float64, device="cuda")
+    st = torch.cuda.current_stream()
+    rc, nt, nh, msg = api.run_device_noalloc(dx.data_ptr(), X.shape[0], X.shape[1], U, y, thr, lt,
+                                             hits.data_ptr(), cap, st.cuda_stream)
+    h = hits.cpu().numpy().view(api.HIT_DTYPE).reshape(-1)[: min(nh, cap)]
+    return rc, nt, np.sort(h, order="kmer"), msg
+
+
+def _existing(X, U, y, thr, lt):
+    with api.Kgwas(precision="split", corr_threshold=thr, log10_thresh=lt) as g:
+        g.set_structure(U, y)
+        return g.run_host(X)
+
+
+def _same(a_hits, b_hits):
+    assert np.array_equal(a_hits["kmer"], b_hits["kmer"])
+    for f in ("effect", "pval", "chisq"):
+        # the relative tolerance of the parity tests against the FP64 oracle
+        assert np.allclose(a_hits[f], b_hits[f], rtol=1e-6, atol=0.0), f
+
+
+def test_noalloc_matches_existing_entry_point_twice():
+    ds = synth.simulate(n=1000, m=20000, S=8, r=16, n_causal=20, missing=0.05, seed=31)
+    X = ds.packed_overlap()
+    ref = _existing(X, ds.U, ds.y, 0.0, 2.0)
+    rc, nt, hits, msg = _device_call(X, ds.U, ds.y, 0.0, 2.0, 4096)
+    assert rc == 0, msg
+    assert nt == ref.n_tested
+    _same(hits, ref.hits)
+
+    ds2 = synth.simulate(n=500, m=7001, S=4, r=6, n_causal=10, missing=0.1, seed=32)
+    X2 = ds2.packed_overlap()
+    ref2 = _existing(X2, ds2.U, ds2.y, 0.2, 1.0)
+    rc, nt, hits, msg = _device_call(X2, ds2.U, ds2.y, 0.2, 1.0, 4096)
+    assert rc == 0, msg
+    assert nt == ref2.n_tested
+    _same(hits, ref2.hits)
+
+
+def test_noalloc_rejects_oversized_structure():
+    # 5000 overlap samples and U with 34 columns: the limb image (5120 x 112) exceeds 256 KiB
+    rng = np.random.default_rng(1)
+    n = 5000
+    U, _ = np.linalg.qr(rng.standard_normal((n, 34)))
+    X = np.zeros((8, synth.words_per_kmer(n)), np.uint64)
+    rc, nt, hits, msg = _device_call(X, U, rng.standard_normal(n), 0.0, 6.0, 16)
+    assert rc == 6, msg  # KG_ERR_UNSUPPORTED
+    assert "maximum" in msg
+
+
+def test_noalloc_reports_short_hit_buffer():
+    ds = synth.simulate(n=200, m=5000, S=4, r=4, n_causal=5, missing=0.0, seed=33)
+    X = ds.packed_overlap()
+    ref = _existing(X, ds.U, ds.y, 0.0, 0.0)      # every tested k-mer is a row
+    rc, nt, hits, msg = _device_call(X, ds.U, ds.y, 0.0, 0.0, 100)
+    assert rc == 1, msg                             # KG_ERR_INVALID, counts still reported
+    assert nt == ref.n_tested and "larger buffer" in msg
+    rc, nt, hits, msg = _device_call(X, ds.U, ds.y, 0.0, 0.0, ref.n_tested)
+    assert rc == 0, msg
+    _same(hits, ref.hits)
