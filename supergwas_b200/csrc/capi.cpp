@@ -66,6 +66,8 @@ struct kg_ctx {
   unsigned long long* dCounters = nullptr;
   kg_hit* dHits = nullptr;
   unsigned long long hit_cap = 0;
+  unsigned long long* dCand = nullptr;  // FP64 refinement candidates (split form)
+  unsigned long long cand_cap = 0;
   uint8_t* dTested = nullptr;
   double* dStat[7] = {};
   size_t stat_cap = 0;
@@ -174,6 +176,7 @@ void kg_destroy(kg_ctx* ctx) {
   dfree(ctx->dBts);
   dfree(ctx->dCounters);
   dfree(ctx->dHits);
+  dfree(ctx->dCand);
   dfree(ctx->dTested);
   for (auto& p : ctx->dStat) dfree(p);
   for (int b = 0; b < NBUF; ++b) {
@@ -222,14 +225,16 @@ int kg_set_structure_ex(kg_ctx* ctx, const double* U, int n, int k, const double
   P.corr_thr = ctx->opts.corr_threshold;
   P.p_thresh = std::pow(10.0, -ctx->opts.log10_thresh);
   P.r2_cand = r2_candidate(P.p_thresh, n);
+  P.thr2_ynorm2 = ctx->opts.corr_threshold * ctx->opts.corr_threshold * p.ynorm * p.ynorm;
   for (int j = 0; j < k; ++j) {
     P.a[j] = p.a[j];
     P.g[j] = p.g[j];
   }
   if (yyM_out) *yyM_out = p.yyM;
   ctx->n_row = n_row;
-  if (ctx->opts.precision == KG_PREC_FP64) {
-    // columns: [count, d_0 .. d_{k-1}, d_y], rows = packed-row sample positions
+  // FP64 columns [count, d_0 .. d_{k-1}, d_y], rows = packed-row sample
+  // positions: the FP64 form's operand, and the split form's refinement operand
+  {
     const int C = k + 2;
     ctx->cm = kg::fp64_cm(C);
     if (ctx->cm < 0) return ctx->fail(KG_ERR_UNSUPPORTED, "too many U.bin columns for the FP64 form");
@@ -243,7 +248,10 @@ int kg_set_structure_ex(kg_ctx* ctx, const double* U, int n, int k, const double
     dfree(ctx->dV);
     KG_CUDA(cudaMalloc((void**)&ctx->dV, V.size() * sizeof(double)), "cudaMalloc(V)");
     KG_CUDA(cudaMemcpy(ctx->dV, V.data(), V.size() * sizeof(double), cudaMemcpyHostToDevice), "copy V");
-  } else {
+  }
+  if (ctx->opts.precision == KG_PREC_SPLIT_I8) {
+    P.refine = 1;
+    P.r2_ref = -std::expm1(-kg::REFINE_CHISQ / (double)n);
     e = kg::make_limbs(p, sample_pos, n_row, ctx->opts.limbs_u, ctx->opts.limbs_y, kg::tc_kc(), ctx->limbs);
     if (!e.empty()) return ctx->fail(KG_ERR_UNSUPPORTED, e);
     if (!kg::tc_supported_n(ctx->limbs.N))
@@ -290,6 +298,15 @@ int ensure_hits(kg_ctx* ctx, unsigned long long cap) {
   return KG_OK;
 }
 
+int ensure_cand(kg_ctx* ctx, unsigned long long cap) {
+  if (ctx->cand_cap >= cap && ctx->dCand) return KG_OK;
+  dfree(ctx->dCand);
+  ctx->cand_cap = 0;
+  KG_CUDA(cudaMalloc((void**)&ctx->dCand, cap * sizeof(unsigned long long)), "cudaMalloc(candidates)");
+  ctx->cand_cap = cap;
+  return KG_OK;
+}
+
 int ensure_stats(kg_ctx* ctx, size_t m) {
   if (ctx->stat_cap >= m && ctx->dTested) return KG_OK;
   dfree(ctx->dTested);
@@ -318,6 +335,8 @@ int launch_one(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, uint64
   O.hits = ctx->dHits;
   O.hit_cap = ctx->hit_cap;
   O.kmer_offset = offset;
+  O.cand = ctx->dCand;
+  O.cand_cap = ctx->cand_cap;
   if (stats) {
     O.tested = ctx->dTested;
     O.chisq = ctx->dStat[0];
@@ -334,6 +353,8 @@ int launch_one(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, uint64
     e = kg::launch_fp64(L, st);
     ctx->last_kernel = "fp64";
   } else {
+    // refinement candidates of this launch start from zero
+    KG_CUDA(cudaMemsetAsync(ctx->dCounters + 3, 0, sizeof(unsigned long long), st), "memset");
     const char* force = std::getenv("KG_KERNEL");
     const bool want_ss = force && std::string(force) == "ss";
     const bool ts_ok = kg::ts_supported(ctx->limbs.N, ctx->opts.limbs_u, ctx->opts.limbs_y, ctx->limbs.Kpad,
@@ -354,11 +375,17 @@ int launch_one(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, uint64
   }
   if (e != cudaSuccess) return ctx->cuda_fail(e, "kernel launch");
   ++ctx->launches;
+  if (ctx->P.refine) {
+    kg::LaunchFp64 R{dx, m, (int)wpk, ctx->dV, ctx->nsteps, ctx->cm, &ctx->P, &O, ctx->num_sms};
+    e = kg::launch_refine(R, st);
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "refinement launch");
+    ++ctx->launches;
+  }
   return KG_OK;
 }
 
 int collect(kg_ctx* ctx, uint64_t m, kg_result* res, kg_stats* st, bool stats_on_device) {
-  if (ctx->counters[2] & ~(unsigned long long)kg::ERR_HIT_OVERFLOW)
+  if (ctx->counters[2] & ~(unsigned long long)(kg::ERR_HIT_OVERFLOW | kg::ERR_CAND_OVERFLOW))
     return ctx->fail(KG_ERR_TIMEOUT, "a bounded device-side wait gave up (error bits " +
                                          std::to_string(ctx->counters[2]) + ")");
   const unsigned long long nh = ctx->counters[1];
@@ -471,11 +498,13 @@ int kg_run_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t wpk, kg
   const bool stats = want_stats(st);
   if (stats && (rc = ensure_stats(ctx, m))) return rc;
   if ((rc = ensure_hits(ctx, std::max<unsigned long long>(ctx->hit_cap, 1ull << 16)))) return rc;
+  if ((rc = ensure_cand(ctx, std::max<unsigned long long>(ctx->cand_cap, 1ull << 20)))) return rc;
   std::memset(ctx->counters, 0, sizeof(ctx->counters));
   if (m) {
     if ((rc = run_host_once(ctx, xbits, m, wpk, stats))) return rc;
-    if (ctx->counters[2] & kg::ERR_HIT_OVERFLOW) {
-      if ((rc = ensure_hits(ctx, ctx->counters[1]))) return rc;
+    for (int retry = 0; retry < 8 && (ctx->counters[2] & (kg::ERR_HIT_OVERFLOW | kg::ERR_CAND_OVERFLOW)); ++retry) {
+      if ((ctx->counters[2] & kg::ERR_HIT_OVERFLOW) && (rc = ensure_hits(ctx, ctx->counters[1]))) return rc;
+      if ((ctx->counters[2] & kg::ERR_CAND_OVERFLOW) && (rc = ensure_cand(ctx, 4 * ctx->cand_cap))) return rc;
       if ((rc = run_host_once(ctx, xbits, m, wpk, stats))) return rc;
     }
   }
@@ -488,6 +517,7 @@ int kg_launch_device(kg_ctx* ctx, const uint64_t* d_x, uint64_t m, uint32_t wpk,
   int rc = check_shape(ctx, d_x, m, wpk);
   if (rc) return rc;
   if ((rc = ensure_hits(ctx, std::max<unsigned long long>(ctx->hit_cap, 1ull << 16)))) return rc;
+  if ((rc = ensure_cand(ctx, std::max<unsigned long long>(ctx->cand_cap, 1ull << 20)))) return rc;
   cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
   ctx->launches = 0;
   KG_CUDA(cudaMemsetAsync(ctx->dCounters, 0, 4 * sizeof(unsigned long long), st), "memset");
@@ -538,9 +568,10 @@ extern "C" int kg_fetch(kg_ctx* ctx, kg_result* res, kg_stats* st) {
                           ctx->pend_stream),
           "copy counters");
   KG_CUDA(cudaStreamSynchronize(ctx->pend_stream), "kernel");
-  if (ctx->counters[2] & kg::ERR_HIT_OVERFLOW) {
-    int rc = ensure_hits(ctx, ctx->counters[1]);
-    if (rc) return rc;
+  for (int retry = 0; retry < 8 && (ctx->counters[2] & (kg::ERR_HIT_OVERFLOW | kg::ERR_CAND_OVERFLOW)); ++retry) {
+    int rc = 0;
+    if ((ctx->counters[2] & kg::ERR_HIT_OVERFLOW) && (rc = ensure_hits(ctx, ctx->counters[1]))) return rc;
+    if ((ctx->counters[2] & kg::ERR_CAND_OVERFLOW) && (rc = ensure_cand(ctx, 4 * ctx->cand_cap))) return rc;
     KG_CUDA(cudaMemsetAsync(ctx->dCounters, 0, 4 * sizeof(unsigned long long), ctx->pend_stream), "memset");
     if ((rc = launch_one(ctx, ctx->pend_x, ctx->pend_m, ctx->pend_wpk, 0, stats, ctx->pend_stream))) return rc;
     KG_CUDA(cudaMemcpyAsync(ctx->counters, ctx->dCounters, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,

@@ -146,40 +146,12 @@ __device__ __forceinline__ double mlog10_sf(double T) {
   return (z * z - log(erfcx(z))) * 0.43429448190325182765;
 }
 
-// Statistics and outputs of one k-mer, given c = popcount(x),
-// ss = sum_j s_j^2, gs = sum_j g_j e_j, ey = d_y . x.  Must be called by
-// all 32 lanes of a warp (warp-aggregated atomics).
-__device__ __forceinline__ void finish_kmer(const EpiParams& P, const DevOut& O, unsigned long long local,
-                                            bool valid, int c, double ss, double gs, double ey) {
-  const int n = P.n;
-  bool tested = valid && c > 0 && c < n && !(P.ynorm < 1e-12);
-  double cor = 0.0;
-  if (tested) {
-    const double xcn2 = (double)c * (double)(n - c) / (double)n;  // ||x - mean x||^2
-    const double xyc = ey + gs + P.kappa * (double)c;              // x . (y - mean y)
-    cor = xyc / (sqrt(xcn2) * P.ynorm);
-    tested = !(fabs(cor) < P.corr_thr);                             // src/kgwas.cpp:199,467
-  }
-  double xxM = 0, xyM = 0, effect = 0, T = 0, p = 1;
-  if (tested) {
-    xxM = (double)c - ss;
-    xyM = P.b * (double)c + ey;
-    // compute_hit, src/kgwas.cpp:44-56
-    const double eps = 1e-12;
-    if (xxM > eps && P.yyM > eps) {
-      double r2 = (xyM * xyM) / (xxM * P.yyM);
-      if (r2 < 0) r2 = 0;
-      if (r2 >= 1) r2 = 1 - 1e-15;
-      if (O.tested || r2 >= P.r2_cand) {
-        T = (double)n * log(1.0 / (1.0 - r2));
-        p = erfc(sqrt(0.5 * T));
-        effect = xyM / (xxM * P.yyM);
-      } else {
-        p = 2.0;  // provably above p_thresh; the row is not emitted and no stats are kept
-      }
-    }
-  }
-  const bool hit = tested && p <= P.p_thresh;
+// Warp-aggregated outputs of one k-mer: tested count, hit record, FP64
+// refinement candidate, and (when requested) the per-k-mer arrays.  All 32
+// lanes of the warp must call it.
+__device__ __forceinline__ void emit_kmer(const DevOut& O, unsigned long long local, bool valid, bool tested,
+                                          bool hit, bool cand, double T, double p, double effect, double xxM,
+                                          double xyM, double cor) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned tmask = __ballot_sync(0xffffffffu, tested);
   if (lane == 0 && tmask) atomicAdd(O.counters + 0, (unsigned long long)__popc(tmask));
@@ -203,6 +175,18 @@ __device__ __forceinline__ void finish_kmer(const EpiParams& P, const DevOut& O,
       }
     }
   }
+  const unsigned cmask = __ballot_sync(0xffffffffu, cand);
+  if (cmask) {
+    unsigned long long base = 0;
+    const int leader = __ffs(cmask) - 1;
+    if ((int)lane == leader) base = atomicAdd(O.counters + 3, (unsigned long long)__popc(cmask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (cand) {
+      const unsigned long long slot = base + __popc(cmask & ((1u << lane) - 1u));
+      if (slot < O.cand_cap) O.cand[slot] = O.kmer_offset + local;
+      else atomicOr(O.counters + 2, (unsigned long long)ERR_CAND_OVERFLOW);
+    }
+  }
   if (valid && O.tested) {
     const unsigned long long g = O.kmer_offset + local;
     O.tested[g] = tested ? 1 : 0;
@@ -214,6 +198,85 @@ __device__ __forceinline__ void finish_kmer(const EpiParams& P, const DevOut& O,
     O.xyM[g] = xyM;
     O.cor[g] = cor;
   }
+}
+
+// Statistics and outputs of one k-mer, given c = popcount(x),
+// ss = sum_j s_j^2, gs = sum_j g_j e_j, ey = d_y . x.  Must be called by
+// all 32 lanes of a warp (warp-aggregated atomics).
+__device__ __forceinline__ void finish_kmer(const EpiParams& P, const DevOut& O, unsigned long long local,
+                                            bool valid, int c, double ss, double gs, double ey) {
+  const int n = P.n;
+  bool tested = valid && c > 0 && c < n && !(P.ynorm < 1e-12);
+  double cor = 0.0;
+  if (tested) {
+    const double xcn2 = (double)c * (double)(n - c) / (double)n;  // ||x - mean x||^2
+    const double xyc = ey + gs + P.kappa * (double)c;              // x . (y - mean y)
+    cor = xyc / (sqrt(xcn2) * P.ynorm);
+    tested = !(fabs(cor) < P.corr_thr);                             // src/kgwas.cpp:199,467
+  }
+  double xxM = 0, xyM = 0, effect = 0, T = 0, p = 1;
+  bool cand = false;
+  if (tested) {
+    xxM = (double)c - ss;
+    xyM = P.b * (double)c + ey;
+    // compute_hit, src/kgwas.cpp:44-56
+    const double eps = 1e-12;
+    if (xxM > eps && P.yyM > eps) {
+      double r2 = (xyM * xyM) / (xxM * P.yyM);
+      if (r2 < 0) r2 = 0;
+      if (r2 >= 1) r2 = 1 - 1e-15;
+      if (P.refine && r2 >= P.r2_ref) {
+        cand = true;  // recomputed in FP64 by refine_kernel, which emits its row
+        p = 2.0;
+      } else if (O.tested || r2 >= P.r2_cand) {
+        T = (double)n * log(1.0 / (1.0 - r2));
+        p = erfc(sqrt(0.5 * T));
+        effect = xyM / (xxM * P.yyM);
+      } else {
+        p = 2.0;  // provably above p_thresh; the row is not emitted and no stats are kept
+      }
+    }
+  }
+  emit_kmer(O, local, valid, tested, tested && p <= P.p_thresh, cand, T, p, effect, xxM, xyM, cor);
+}
+
+
+// As finish_kmer, for launches without per-k-mer outputs: the Pearson gate
+// and the emit / refinement screens compare squares instead of dividing
+// (|cor| >= thr  <=>  xyc^2 >= thr^2 ||xc||^2 ||yc||^2;  r2 >= t  <=>
+// xyM^2 >= t xxM yyM), and only k-mers that may reach the emit cut evaluate
+// the reference formula (src/kgwas.cpp:47-53) exactly.
+__device__ __forceinline__ void finish_kmer_fast(const EpiParams& P, const DevOut& O, unsigned long long local,
+                                                 bool valid, int c, double ss, double gs, double ey) {
+  const int n = P.n;
+  bool tested = valid && c > 0 && c < n && !(P.ynorm < 1e-12);
+  if (tested && P.corr_thr > 0.0) {
+    const double xcn2 = (double)c * (double)(n - c) / (double)n;
+    const double xyc = ey + gs + P.kappa * (double)c;
+    tested = xyc * xyc >= P.thr2_ynorm2 * xcn2;
+  }
+  double xxM = 0, xyM = 0, effect = 0, T = 0, p = 1;
+  bool cand = false, hit = false;
+  if (tested) {
+    xxM = (double)c - ss;
+    xyM = P.b * (double)c + ey;
+    const double eps = 1e-12;
+    if (xxM > eps && P.yyM > eps) {
+      const double q = xyM * xyM, den = xxM * P.yyM;
+      if (P.refine && q >= P.r2_ref * den) {
+        cand = true;
+      } else if (q >= P.r2_cand * den) {
+        double r2 = q / den;
+        if (r2 < 0) r2 = 0;
+        if (r2 >= 1) r2 = 1 - 1e-15;
+        T = (double)n * log(1.0 / (1.0 - r2));
+        p = erfc(sqrt(0.5 * T));
+        effect = xyM / den;
+        hit = p <= P.p_thresh;
+      }
+    }
+  }
+  emit_kmer(O, local, valid, tested, hit, cand, T, p, effect, xxM, xyM, 0.0);
 }
 
 }  // namespace kg

@@ -1,18 +1,19 @@
 // kernel_ts.cu -- split-precision association kernel with the unpacked x
 // operand held in tensor memory.
 //
-// One persistent CTA per SM, warp-specialised (448 threads):
-//   warps 0-3   epilogue: tcgen05.ld of the int32 accumulators (one TMEM lane
-//               = one k-mer), exact limb recombination, FP64 statistics,
-//               warp-aggregated hit compaction;
-//   warps 4-11  unpack, two groups of four (one warp per TMEM lane quarter):
+// One persistent CTA per SM, warp-specialised (576 threads):
+//   warps 0-7   epilogue, two groups of four, group g owning TMEM accumulator
+//               g (tiles alternate between them): tcgen05.ld of the int32
+//               accumulators (one TMEM lane = one k-mer), limb recombination,
+//               FP64 statistics, warp-aggregated hit compaction;
+//   warps 8-15  unpack, two groups of four (one warp per TMEM lane quarter):
 //               read 128 samples of a packed row from the TMA-filled shared
 //               tile and write them as int8 (0 / -128) straight into a TMEM
 //               A stage with tcgen05.st -- the unpacked operand never touches
 //               shared memory;
-//   warp 12     producer: one 2-D TMA load (128 rows x 128 bytes, 128-byte
+//   warp 16     producer: one 2-D TMA load (128 rows x 128 bytes, 128-byte
 //               swizzle, no multicast) per 1024 samples of a 128-k-mer tile;
-//   warp 13     MMA: tcgen05.mma kind::i8, A from TMEM, B (the int8 limbs of
+//   warp 17     MMA: tcgen05.mma kind::i8, A from TMEM, B (the int8 limbs of
 //               the centred structure and phenotype columns, resident in
 //               shared memory for the whole launch) from a smem descriptor,
 //               accumulating into one of two TMEM accumulators.
@@ -36,10 +37,10 @@ constexpr int TS_TM = 128;
 constexpr int TS_KS = 128;         // samples per A stage
 constexpr int TS_BOX = 1024;       // samples per TMA box (128 bytes)
 constexpr int TS_XST = 4;          // packed boxes in flight
-constexpr int TS_THREADS = 448;
+constexpr int TS_THREADS = 576;
 constexpr int TS_LU = 3, TS_LY = 5;
 constexpr uint32_t TS_XBYTES = TS_TM * 128;  // one box: 128 rows x 128 bytes
-constexpr int TS_WARP_PROD = 12, TS_WARP_MMA = 13;
+constexpr int TS_WARP_UNPACK0 = 8, TS_WARP_PROD = 16, TS_WARP_MMA = 17;
 
 __host__ __device__ constexpr int ts_a0(int N) { return ((2 * N + 31) / 32) * 32; }
 __host__ __device__ constexpr int ts_ast(int N) {
@@ -211,9 +212,9 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
       tc_commit(drain);
       mbar_wait(drain, 0, O.counters, ERR_TIMEOUT_MMA);
     }
-  } else if (warp >= 4) {
+  } else if (warp >= TS_WARP_UNPACK0) {
     // -------------------------------------------------------------- unpack
-    const int grp = (warp - 4) >> 2;           // 0 or 1
+    const int grp = (warp - TS_WARP_UNPACK0) >> 2;  // 0 or 1
     const int q = warp & 3;                    // TMEM lane quarter
     const int r = q * 32 + lane;               // row of the tile = TMEM lane
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
@@ -261,11 +262,14 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     }
   } else {
     // ------------------------------------------------------------ epilogue
-    const int r = warp * 32 + lane;
-    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    const int eg = warp >> 2;                  // group = accumulator buffer
+    const int q = warp & 3;
+    const int r = q * 32 + lane;
+    const uint32_t lane_base = (uint32_t)(q * 32) << 16;
     uint32_t i = 0;
     for (unsigned long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
-      const uint32_t b = i & 1, v = i >> 1;
+      if ((int)(i & 1) != eg) continue;
+      const uint32_t b = eg, v = i >> 1;
       if (!__all_sync(0xffffffffu, ts_wait(acc_full + 8 * b, v & 1, s_abort, O.counters, ERR_TIMEOUT_MMA))) break;
       tc_fence_after();
       uint32_t d[N];
@@ -282,12 +286,14 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
       if (lane == 0) mbar_arrive(acc_empty + 8 * b);
       const unsigned long long local = tile * TS_TM + r;
       const bool valid = local < m;
-      // accumulators hold -128 * (integer sums); recombine limbs exactly
-      const int c = -((int)d[0]) >> 7;
-      long long vy = 0;
+      // accumulators hold -128 * (integer limb sums): divide the 128 out in
+      // integers (exact), then recombine the limbs in FP64 (exact: the value
+      // stays below 2^53), so the result equals the smem-A kernel's bit for bit
+      const int c = (-(int)d[0]) >> 7;
+      double vy = (double)((-(int)d[1]) >> 7);
 #pragma unroll
-      for (int l = 0; l < TS_LY; ++l) vy = vy * 256 + (long long)(int)d[1 + l];
-      const double ey = -(double)vy * (LM.scale[P.k] * 0.0078125);
+      for (int l = 1; l < TS_LY; ++l) vy = fma(vy, 256.0, (double)((-(int)d[1 + l]) >> 7));
+      const double ey = vy * LM.scale[P.k];
       double ss = 0, gs = 0;
       if (DROP0) {
         const double s0 = P.a[0] * (double)c;
@@ -297,16 +303,18 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
       for (int jj = 0; jj < KU_MAX; ++jj) {
         const int j = jj + (DROP0 ? 1 : 0);
         if (j < P.k) {
-          long long vj = 0;
+          const int o = 1 + TS_LY + TS_LU * jj;
+          double vj = (double)((-(int)d[o]) >> 7);
 #pragma unroll
-          for (int l = 0; l < TS_LU; ++l) vj = vj * 256 + (long long)(int)d[1 + TS_LY + TS_LU * jj + l];
-          const double e = -(double)vj * (LM.scale[j] * 0.0078125);
-          const double sj = P.a[j] * (double)c + e;
-          ss += sj * sj;
-          gs += P.g[j] * e;
+          for (int l = 1; l < TS_LU; ++l) vj = fma(vj, 256.0, (double)((-(int)d[o + l]) >> 7));
+          const double e = vj * LM.scale[j];
+          const double sj = fma(P.a[j], (double)c, e);
+          ss = fma(sj, sj, ss);
+          gs = fma(P.g[j], e, gs);
         }
       }
-      finish_kmer(P, O, local, valid, c, ss, gs, ey);
+      if (O.tested) finish_kmer(P, O, local, valid, c, ss, gs, ey);
+      else finish_kmer_fast(P, O, local, valid, c, ss, gs, ey);
     }
   }
   __syncthreads();

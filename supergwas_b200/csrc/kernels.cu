@@ -121,6 +121,114 @@ cudaError_t launch_fp64(const LaunchFp64& L, cudaStream_t st) {
   }
 }
 
+// ====================================================== FP64 refinement pass
+// One warp per candidate k-mer (chi-square >= REFINE_CHISQ in the split form):
+// the lanes walk the set bits of the packed row, add the FP64 contraction
+// columns (same layout as the FP64 form), reduce across the warp, and lane 0
+// evaluates compute_hit (src/kgwas.cpp:44-56) and emits the row.
+template <int CM>
+__global__ void __launch_bounds__(256) refine_kernel(const uint64_t* __restrict__ x, int wpk,
+                                                     const double* __restrict__ V, int vrows,
+                                                     const __grid_constant__ EpiParams P, const DevOut O) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x >> 5);
+  unsigned long long ncand = O.counters[3];
+  if (ncand > O.cand_cap) ncand = O.cand_cap;
+  for (unsigned long long w = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < ncand;
+       w += warps) {
+    const unsigned long long g = O.cand[w];
+    const uint64_t* row = x + (g - O.kmer_offset) * (unsigned long long)wpk;
+    double acc[CM];
+#pragma unroll
+    for (int j = 0; j < CM; ++j) acc[j] = 0.0;
+    for (int wi = lane; wi < wpk; wi += 32) {
+      uint64_t bits = __ldg(row + wi);
+      while (bits) {
+        const int b = __ffsll((long long)bits) - 1;
+        bits &= bits - 1;
+        const int smp = wi * 64 + b;
+        if (smp < vrows) {
+          const double* v = V + (size_t)smp * CM;
+#pragma unroll
+          for (int j = 0; j < CM; ++j) acc[j] += v[j];
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < CM; ++j)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+    if (lane == 0) {
+      const int c = (int)acc[0];
+      double ss = 0, ey = 0;
+#pragma unroll
+      for (int j = 1; j < CM; ++j) {
+        if (j <= P.k) {
+          const double sj = P.a[j - 1] * (double)c + acc[j];
+          ss += sj * sj;
+        } else if (j == P.k + 1) {
+          ey = acc[j];
+        }
+      }
+      const double xxM = (double)c - ss, xyM = P.b * (double)c + ey;
+      double effect = 0, T = 0, p = 1;
+      const double eps = 1e-12;
+      if (xxM > eps && P.yyM > eps) {
+        double r2 = (xyM * xyM) / (xxM * P.yyM);
+        if (r2 < 0) r2 = 0;
+        if (r2 >= 1) r2 = 1 - 1e-15;
+        T = (double)P.n * log(1.0 / (1.0 - r2));
+        p = erfc(sqrt(0.5 * T));
+        effect = xyM / (xxM * P.yyM);
+      }
+      if (p <= P.p_thresh) {
+        const unsigned long long slot = atomicAdd(O.counters + 1, 1ull);
+        if (slot < O.hit_cap) {
+          kg_hit h;
+          h.kmer = g;
+          h.effect = effect;
+          h.pval = p;
+          h.chisq = T;
+          O.hits[slot] = h;
+        } else {
+          atomicOr(O.counters + 2, (unsigned long long)ERR_HIT_OVERFLOW);
+        }
+      }
+      if (O.tested) {
+        O.chisq[g] = T;
+        O.pval[g] = p;
+        O.effect[g] = effect;
+        O.mlog10p[g] = mlog10_sf(T);
+        O.xxM[g] = xxM;
+        O.xyM[g] = xyM;
+      }
+    }
+  }
+}
+
+template <int CM>
+static cudaError_t launch_refine_t(const LaunchFp64& L, cudaStream_t st) {
+  const unsigned grid = (unsigned)(L.num_sms * 4);
+  refine_kernel<CM><<<grid, 256, 0, st>>>(L.x, L.wpk, L.V, L.nsteps * F64_SCH, *L.P, *L.O);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_refine(const LaunchFp64& L, cudaStream_t st) {
+  switch (L.cm) {
+    case 8: return launch_refine_t<8>(L, st);
+    case 12: return launch_refine_t<12>(L, st);
+    case 16: return launch_refine_t<16>(L, st);
+    case 20: return launch_refine_t<20>(L, st);
+    case 24: return launch_refine_t<24>(L, st);
+    case 28: return launch_refine_t<28>(L, st);
+    case 36: return launch_refine_t<36>(L, st);
+    case 44: return launch_refine_t<44>(L, st);
+    case 52: return launch_refine_t<52>(L, st);
+    case 68: return launch_refine_t<68>(L, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 // ============================================== tcgen05 kind::i8, A from SMEM
 constexpr int TC_TM = 128;   // k-mers per tile (MMA M)
 constexpr int TC_KC = 256;   // samples per K chunk
@@ -252,9 +360,9 @@ __global__ void __launch_bounds__(TC_TM, 1)
       for (int l = 0; l < LM.nl[j]; ++l) v = v * 256 + (long long)d[LM.first[j] + l];
       const double e = (double)v * LM.scale[j];
       if (j < P.k) {
-        const double sj = P.a[j] * (double)c + e;
-        ss += sj * sj;
-        gs += P.g[j] * e;
+        const double sj = fma(P.a[j], (double)c, e);
+        ss = fma(sj, sj, ss);
+        gs = fma(P.g[j], e, gs);
       } else {
         ey = e;
       }

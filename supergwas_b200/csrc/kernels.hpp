@@ -32,6 +32,8 @@ struct LaunchTc {
 int fp64_cm(int C);           // padded column count for C contraction columns (-1: too many)
 int fp64_steps(int n);        // 128-sample steps covering n samples
 cudaError_t launch_fp64(const LaunchFp64& L, cudaStream_t st);
+// FP64 recomputation of the split form's refinement candidates (same V layout).
+cudaError_t launch_refine(const LaunchFp64& L, cudaStream_t st);
 
 struct LaunchTs {
   const uint64_t* x;          // packed rows (device), 16-byte aligned

@@ -12,6 +12,9 @@ struct EpiParams {
   int n, k;
   double b, kappa, yyM, ynorm, corr_thr, p_thresh;
   double r2_cand;   // r2 below this cannot give p <= p_thresh (log/erfc skipped)
+  int refine;       // 1: k-mers with r2 >= r2_ref go to the FP64 refinement list
+  double r2_ref;
+  double thr2_ynorm2;  // corr_thr^2 * ynorm^2 (division-free Pearson gate)
   double a[KMAX];
   double g[KMAX];
 };
@@ -26,15 +29,23 @@ struct LimbMap {
 
 // Device outputs of one launch.
 struct DevOut {
-  unsigned long long* counters;  // [0] tested, [1] hits, [2] error bits
+  unsigned long long* counters;  // [0] tested, [1] hits, [2] error bits, [3] refinement candidates
   kg_hit* hits;
   unsigned long long hit_cap;
   unsigned long long kmer_offset;  // added to the launch-local k-mer index
   // optional per-k-mer arrays, indexed by kmer_offset + local index
   uint8_t* tested;
   double *chisq, *pval, *effect, *mlog10p, *xxM, *xyM, *cor;
+  // FP64 refinement list (global k-mer indices), used when EpiParams::refine
+  unsigned long long* cand;
+  unsigned long long cand_cap;
 };
 
-enum : unsigned { ERR_TIMEOUT_FULL = 1u, ERR_TIMEOUT_MMA = 2u, ERR_HIT_OVERFLOW = 4u };
+enum : unsigned { ERR_TIMEOUT_FULL = 1u, ERR_TIMEOUT_MMA = 2u, ERR_HIT_OVERFLOW = 4u, ERR_CAND_OVERFLOW = 8u };
+
+// Chi-square above which the split form hands a k-mer to the FP64
+// refinement kernel: there -log10 p ~ T / (2 ln 10) grows with T, so an
+// absolute 1e-6 bound needs FP64 accuracy; below it 24-bit U limbs suffice.
+constexpr double REFINE_CHISQ = 12.0;
 
 }  // namespace kg

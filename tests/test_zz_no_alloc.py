@@ -38,10 +38,13 @@ def _existing(X, U, y, thr, lt):
 
 
 def _same(a_hits, b_hits):
+    """Same rows; values within the parity tests' tolerances (chi-square and
+    effect 1e-6 relative, -log10 p 1e-6 absolute)."""
+    from oracle import oracle as O
     assert np.array_equal(a_hits["kmer"], b_hits["kmer"])
-    for f in ("effect", "pval", "chisq"):
-        # the relative tolerance of the parity tests against the FP64 oracle
+    for f in ("effect", "chisq"):
         assert np.allclose(a_hits[f], b_hits[f], rtol=1e-6, atol=0.0), f
+    assert np.all(np.abs(O.mlog10p(a_hits["chisq"]) - O.mlog10p(b_hits["chisq"])) <= 1e-6)
 
 
 def test_noalloc_matches_existing_entry_point_twice():
