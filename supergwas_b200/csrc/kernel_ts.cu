@@ -1,19 +1,20 @@
 // kernel_ts.cu -- split-precision association kernel with the unpacked x
 // operand held in tensor memory.
 //
-// One persistent CTA per SM, warp-specialised (576 threads):
-//   warps 0-7   epilogue, two groups of four, group g owning TMEM accumulator
-//               g (tiles alternate between them): tcgen05.ld of the int32
-//               accumulators (one TMEM lane = one k-mer), limb recombination,
-//               FP64 statistics, warp-aggregated hit compaction;
-//   warps 8-15  unpack, two groups of four (one warp per TMEM lane quarter):
+// One persistent CTA per SM, warp-specialised (704 threads):
+//   warps 0-3   epilogue: tcgen05.ld of the int32 accumulators (one TMEM lane
+//               = one k-mer), limb recombination, FP64 statistics,
+//               warp-aggregated hit compaction;
+//   warps 4-19  unpack, four groups of four (one warp per TMEM lane quarter),
+//               the groups taking K stages in turn so that four stores to
+//               tensor memory are in flight per lane quarter:
 //               read 128 samples of a packed row from the TMA-filled shared
 //               tile and write them as int8 (0 / -128) straight into a TMEM
 //               A stage with tcgen05.st -- the unpacked operand never touches
 //               shared memory;
-//   warp 16     producer: one 2-D TMA load (128 rows x 128 bytes, 128-byte
+//   warp 20     producer: one 2-D TMA load (128 rows x 128 bytes, 128-byte
 //               swizzle, no multicast) per 1024 samples of a 128-k-mer tile;
-//   warp 17     MMA: tcgen05.mma kind::i8, A from TMEM, B (the int8 limbs of
+//   warp 21     MMA: tcgen05.mma kind::i8, A from TMEM, B (the int8 limbs of
 //               the centred structure and phenotype columns, resident in
 //               shared memory for the whole launch) from a smem descriptor,
 //               accumulating into one of two TMEM accumulators.
@@ -37,10 +38,11 @@ constexpr int TS_TM = 128;
 constexpr int TS_KS = 128;         // samples per A stage
 constexpr int TS_BOX = 1024;       // samples per TMA box (128 bytes)
 constexpr int TS_XST = 4;          // packed boxes in flight
-constexpr int TS_THREADS = 576;
+constexpr int TS_UG = 4;           // unpack groups
+constexpr int TS_THREADS = 32 * (4 + 4 * TS_UG + 2);
 constexpr int TS_LU = 3, TS_LY = 5;
 constexpr uint32_t TS_XBYTES = TS_TM * 128;  // one box: 128 rows x 128 bytes
-constexpr int TS_WARP_UNPACK0 = 8, TS_WARP_PROD = 16, TS_WARP_MMA = 17;
+constexpr int TS_WARP_UNPACK0 = 4, TS_WARP_PROD = 4 + 4 * TS_UG, TS_WARP_MMA = TS_WARP_PROD + 1;
 
 __host__ __device__ constexpr int ts_a0(int N) { return ((2 * N + 31) / 32) * 32; }
 __host__ __device__ constexpr int ts_ast(int N) {
@@ -127,7 +129,7 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
   if (tid == 32) {
     for (int s = 0; s < TS_XST; ++s) {
       mbar_init(x_full + 8 * s, 1);
-      mbar_init(x_empty + 8 * s, 8);  // 4 warps x 2 unpack groups
+      mbar_init(x_empty + 8 * s, 4 * TS_UG);  // every unpack warp
     }
     for (int t = 0; t < AST; ++t) {
       mbar_init(a_full + 8 * t, 4);   // the 4 warps of one unpack group
@@ -214,7 +216,7 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     }
   } else if (warp >= TS_WARP_UNPACK0) {
     // -------------------------------------------------------------- unpack
-    const int grp = (warp - TS_WARP_UNPACK0) >> 2;  // 0 or 1
+    const int grp = (warp - TS_WARP_UNPACK0) >> 2;  // 0 .. TS_UG-1
     const int q = warp & 3;                    // TMEM lane quarter
     const int r = q * 32 + lane;               // row of the tile = TMEM lane
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
@@ -231,7 +233,7 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
         const int kc0 = bx * (TS_BOX / TS_KS);
         const int kc1 = kc0 + TS_BOX / TS_KS < nchunk ? kc0 + TS_BOX / TS_KS : nchunk;
         for (int kc = kc0; kc < kc1; ++kc, ++g) {
-          if ((int)(g & 1) != grp) continue;
+          if ((int)(g % TS_UG) != grp) continue;
           const uint32_t t = g % AST, u = g / AST;
           if (u > 0 && !__all_sync(0xffffffffu, ts_wait(a_empty + 8 * t, (u - 1) & 1, s_abort, O.counters,
                                                         ERR_TIMEOUT_MMA))) {
@@ -246,10 +248,13 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
                        : "r"(sx + s * TS_XBYTES + r * 128 + ((c ^ (r & 7)) << 4)));
           const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
           uint32_t o[32];
+          // byte t of column 8qq+j = bit 8t+j of word qq, moved to the byte's
+          // sign bit (0 or -128); the shift is a multiply so that it issues on
+          // the FMA pipe and the mask on the ALU pipe
 #pragma unroll
           for (int qq = 0; qq < 4; ++qq)
 #pragma unroll
-            for (int j = 0; j < 8; ++j) o[qq * 8 + j] = (w4[qq] << (7 - j)) & 0x80808080u;  // 0 or -128
+            for (int j = 0; j < 8; ++j) o[qq * 8 + j] = (w4[qq] * (1u << (7 - j))) & 0x80808080u;
           tc_st32(tmem + lane_base + A0 + t * 32, o);
           tc_wait_st();
           tc_fence_before();
@@ -262,14 +267,12 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     }
   } else {
     // ------------------------------------------------------------ epilogue
-    const int eg = warp >> 2;                  // group = accumulator buffer
     const int q = warp & 3;
     const int r = q * 32 + lane;
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
     uint32_t i = 0;
     for (unsigned long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
-      if ((int)(i & 1) != eg) continue;
-      const uint32_t b = eg, v = i >> 1;
+      const uint32_t b = i & 1, v = i >> 1;
       if (!__all_sync(0xffffffffu, ts_wait(acc_full + 8 * b, v & 1, s_abort, O.counters, ERR_TIMEOUT_MMA))) break;
       tc_fence_after();
       uint32_t d[N];
