@@ -138,6 +138,59 @@ int kg_launch_device_stats(kg_ctx* ctx, const uint64_t* d_xbits, uint64_t n_kmer
 void* kg_host_alloc(size_t bytes);
 void kg_host_free(void* p);
 
+/* ---------------------------------------------------------------------
+ * Many phenotypes over one batch.  The reference runs one kgwas process per
+ * (phenotype, batch) pair (HPC/kgwas/kgwas_cols.sh:22-65), each re-reading
+ * the batch; here one launch tests every phenotype against each k-mer tile
+ * while the tile's packed rows stay on chip.  Rows hold n_row_samples
+ * samples (e.g. all of samples.txt); phenotype p has its own overlap
+ * (sample_pos, n), U.bin (U, k) and y, as if its own kgwas process had run
+ * build_overlap + load_Ubin on it (src/kgwas_utils.hpp:129-157, 285-314).
+ * The batch may be the concatenation of several shards (batch_* of uneven
+ * length): tested counts are kept per shard, as the reference's .count
+ * files are (src/kgwas.cpp:291-304).
+ * ------------------------------------------------------------------- */
+typedef struct kg_pheno {
+    const double* U_colmajor;  /* n x k, column-major                          */
+    int n;                     /* overlap samples of this phenotype            */
+    int k;                     /* U.bin columns                                */
+    const double* y;           /* n phenotype values, in row-position order    */
+    const int32_t* sample_pos; /* bit position of overlap sample i in each row */
+} kg_pheno;
+
+typedef struct kg_phit {
+    uint64_t kmer;     /* index within the launch's rows                       */
+    int32_t pheno;     /* phenotype index                                      */
+    int32_t shard;     /* shard index                                          */
+    double effect;
+    double pval;
+    double chisq;
+} kg_phit;
+
+typedef struct kg_multi_result {
+    uint64_t n_kmers;
+    int n_pheno;
+    int n_shards;
+    const uint64_t* n_tested;  /* [shard * n_pheno + pheno]: the .count values */
+    uint64_t n_hits;
+    const kg_phit* hits;       /* sorted by (pheno, kmer); owned by the context */
+} kg_multi_result;
+
+/* Set the phenotypes of a context (split precision only). */
+int kg_set_phenotypes(kg_ctx* ctx, const kg_pheno* phenos, int n_pheno, int n_row_samples);
+
+/* Test every phenotype on device rows.  shard_start (host, n_shards entries,
+ * ascending, shard_start[0] = 0) splits the rows into shards; NULL = one
+ * shard.  Asynchronous on `stream` until kg_fetch_multi. */
+int kg_launch_multi_device(kg_ctx* ctx, const uint64_t* d_xbits, uint64_t n_kmers,
+                           uint32_t words_per_kmer, const uint64_t* shard_start, int n_shards,
+                           void* stream);
+int kg_fetch_multi(kg_ctx* ctx, kg_multi_result* res);
+
+/* Same from host rows (chunked host-to-device copies overlapped with the kernels). */
+int kg_run_multi_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t n_kmers, uint32_t words_per_kmer,
+                      const uint64_t* shard_start, int n_shards, kg_multi_result* res);
+
 /* Number of kernel launches the last kg_run_host / kg_launch_device made. */
 int kg_last_launch_count(const kg_ctx* ctx);
 

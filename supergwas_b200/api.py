@@ -56,6 +56,20 @@ class _Stats(ctypes.Structure):
 
 STAT_FIELDS = ("chisq", "pval", "effect", "mlog10p", "xxM", "xyM", "cor")
 
+PHIT_DTYPE = np.dtype([("kmer", np.uint64), ("pheno", np.int32), ("shard", np.int32), ("effect", np.float64),
+                       ("pval", np.float64), ("chisq", np.float64)])
+
+
+class _Pheno(ctypes.Structure):
+    _fields_ = [("U_colmajor", _DP), ("n", ctypes.c_int), ("k", ctypes.c_int), ("y", _DP),
+                ("sample_pos", ctypes.c_void_p)]
+
+
+class _MultiResult(ctypes.Structure):
+    _fields_ = [("n_kmers", ctypes.c_uint64), ("n_pheno", ctypes.c_int), ("n_shards", ctypes.c_int),
+                ("n_tested", ctypes.POINTER(ctypes.c_uint64)), ("n_hits", ctypes.c_uint64),
+                ("hits", ctypes.c_void_p)]
+
 _LIB = None
 
 
@@ -98,6 +112,11 @@ def lib():
     L.kg_host_alloc.restype = vp
     L.kg_host_free.argtypes = [vp]
     L.kg_host_free.restype = None
+    L.kg_set_phenotypes.argtypes = [vp, ctypes.POINTER(_Pheno), ctypes.c_int, ctypes.c_int]
+    L.kg_launch_multi_device.argtypes = [vp, vp, ctypes.c_uint64, ctypes.c_uint32, vp, ctypes.c_int, vp]
+    L.kg_fetch_multi.argtypes = [vp, ctypes.POINTER(_MultiResult)]
+    L.kg_run_multi_host.argtypes = [vp, vp, ctypes.c_uint64, ctypes.c_uint32, vp, ctypes.c_int,
+                                    ctypes.POINTER(_MultiResult)]
     L.kg_run_device_noalloc.argtypes = [vp, ctypes.c_uint64, ctypes.c_uint32, _DP, ctypes.c_int, ctypes.c_int,
                                         _DP, ctypes.c_double, ctypes.c_double, vp, ctypes.c_uint64,
                                         ctypes.POINTER(ctypes.c_uint64), vp, ctypes.c_char_p, ctypes.c_size_t]
@@ -228,6 +247,59 @@ class Kgwas:
         self._check(self._L.kg_fetch(self._h, ctypes.byref(r), ctypes.byref(st) if st is not None else None),
                     "kg_fetch")
         return self._result(r, arrs)
+
+    # ---------------------------------------------------- many phenotypes
+    def set_phenotypes(self, phenos, n_row_samples: int):
+        """phenos: list of (U (n x k), y (n), sample_pos (n)) sharing one row layout."""
+        keep = []
+        arr = (_Pheno * len(phenos))()
+        for i, (U, y, pos) in enumerate(phenos):
+            U = np.asarray(U, dtype=np.float64)
+            Uc = np.ascontiguousarray(U.T)
+            yv = np.ascontiguousarray(y, dtype=np.float64)
+            pv = np.ascontiguousarray(pos, dtype=np.int32)
+            keep += [Uc, yv, pv]
+            arr[i].U_colmajor = Uc.ctypes.data_as(_DP)
+            arr[i].n = U.shape[0]
+            arr[i].k = U.shape[1]
+            arr[i].y = yv.ctypes.data_as(_DP)
+            arr[i].sample_pos = pv.ctypes.data
+        self._check(self._L.kg_set_phenotypes(self._h, arr, len(phenos), int(n_row_samples)), "kg_set_phenotypes")
+        self._np = len(phenos)
+
+    def _multi_result(self, r):
+        nh = int(r.n_hits)
+        hits = np.zeros(nh, PHIT_DTYPE)
+        if nh:
+            hits = np.frombuffer(ctypes.string_at(r.hits, nh * PHIT_DTYPE.itemsize), dtype=PHIT_DTYPE).copy()
+        ns, npn = int(r.n_shards), int(r.n_pheno)
+        tested = np.ctypeslib.as_array(r.n_tested, shape=(ns * npn,)).copy().reshape(ns, npn)
+        return tested, hits
+
+    @staticmethod
+    def _shards(shard_start):
+        if shard_start is None:
+            return None, 0, None
+        a = np.ascontiguousarray(shard_start, dtype=np.uint64)
+        return a.ctypes.data, a.shape[0], a
+
+    def launch_multi_device(self, dptr: int, m: int, wpk: int, shard_start=None, stream: int | None = None):
+        sp, ns, keep = self._shards(shard_start)
+        self._check(self._L.kg_launch_multi_device(self._h, dptr, m, wpk, sp, ns, stream), "kg_launch_multi_device")
+
+    def fetch_multi(self):
+        """Returns (tested counts [n_shards, n_pheno], hits PHIT_DTYPE sorted by (pheno, kmer))."""
+        r = _MultiResult()
+        self._check(self._L.kg_fetch_multi(self._h, ctypes.byref(r)), "kg_fetch_multi")
+        return self._multi_result(r)
+
+    def run_multi_host(self, packed: np.ndarray, shard_start=None):
+        packed = np.ascontiguousarray(packed, dtype=np.uint64)
+        sp, ns, keep = self._shards(shard_start)
+        r = _MultiResult()
+        self._check(self._L.kg_run_multi_host(self._h, packed.ctypes.data, packed.shape[0], packed.shape[1],
+                                              sp, ns, ctypes.byref(r)), "kg_run_multi_host")
+        return self._multi_result(r)
 
     def last_launch_count(self) -> int:
         return int(self._L.kg_last_launch_count(self._h))

@@ -22,7 +22,7 @@ LIB = os.path.join(LIB_DIR, "libkgwas_cuda.so")
 CLI = os.path.join(BIN_DIR, "kgwas")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-LIB_SOURCES = ["kernels.cu", "kernel_ts.cu", "noalloc.cu", "capi.cpp", "prep.cpp"]
+LIB_SOURCES = ["kernels.cu", "kernel_ts.cu", "kernel_mp.cu", "noalloc.cu", "capi.cpp", "capi_multi.cpp", "prep.cpp"]
 CLI_SOURCES = ["kgwas_main.cpp", "kgwas_io.cpp"]
 
 

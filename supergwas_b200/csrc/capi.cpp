@@ -15,95 +15,9 @@
 
 #define KG_VERSION "kgwas-b200 0.1.0"
 
-namespace {
+#include "ctx.hpp"
 
-constexpr int NBUF = 2;  // host-run chunk buffers in flight
-
-// Smallest r2 that can still give p = erfc(sqrt(T/2)) <= p_thresh with
-// T = n log(1/(1-r2)) (src/kgwas.cpp:51-52), lowered by a relative margin of
-// 1e-9 so that k-mers below it are certainly not emitted.  -1 when every
-// tested k-mer may be emitted.
-double r2_candidate(double p_thresh, int n) {
-  if (!(p_thresh < 1.0)) return -1.0;
-  if (p_thresh <= 0.0) return 2.0;
-  double lo = 0.0, hi = 1.0;
-  while (std::erfc(std::sqrt(0.5 * hi)) > p_thresh && hi < 1e7) hi *= 2;
-  for (int it = 0; it < 200; ++it) {
-    const double mid = 0.5 * (lo + hi);
-    if (std::erfc(std::sqrt(0.5 * mid)) > p_thresh) lo = mid; else hi = mid;
-  }
-  const double T = lo;  // erfc(sqrt(T/2)) > p_thresh for every T < lo
-  const double r2 = -std::expm1(-T / (double)n);
-  return r2 * (1.0 - 1e-9);
-}
-
-template <class T>
-void dfree(T*& p) {
-  if (p) cudaFree((void*)p);
-  p = nullptr;
-}
-
-}  // namespace
-
-struct kg_ctx {
-  kg_opts opts{};
-  int num_sms = 0;
-  cudaStream_t stream = nullptr, copy_stream = nullptr;
-  std::string err;
-  bool have_structure = false;
-  int n_row = 0;  // samples per packed row
-  kg::Prepared prep;
-  kg::LimbCols limbs;
-  kg::EpiParams P{};
-  kg::LimbMap LM{};
-  // structure on the device
-  double* dV = nullptr;
-  int cm = 0, nsteps = 0;
-  int8_t* dB = nullptr;      // B image of the smem-A kernel
-  int8_t* dBts = nullptr;    // B image of the TMEM-A kernel
-  int nchunk = 0;
-  // outputs on the device
-  unsigned long long* dCounters = nullptr;
-  kg_hit* dHits = nullptr;
-  unsigned long long hit_cap = 0;
-  unsigned long long* dCand = nullptr;  // FP64 refinement candidates (split form)
-  unsigned long long cand_cap = 0;
-  uint8_t* dTested = nullptr;
-  double* dStat[7] = {};
-  size_t stat_cap = 0;
-  // host result
-  std::vector<kg_hit> hits;
-  unsigned long long counters[3] = {0, 0, 0};
-  // pending device launch
-  bool pending = false;
-  const uint64_t* pend_x = nullptr;
-  uint64_t pend_m = 0;
-  uint32_t pend_wpk = 0;
-  bool pend_stats = false;
-  cudaStream_t pend_stream = nullptr;
-  int launches = 0;
-  const char* last_kernel = "";
-  // host-run buffers
-  uint64_t* dChunk[NBUF] = {};
-  void* hStage[NBUF] = {};
-  size_t chunk_bytes = 0;
-  cudaEvent_t ev_h2d[NBUF] = {}, ev_k[NBUF] = {};
-
-  int fail(int code, const std::string& m) {
-    err = m;
-    return code;
-  }
-  int cuda_fail(cudaError_t e, const char* what) {
-    err = std::string(what) + ": " + cudaGetErrorString(e);
-    return KG_ERR_CUDA;
-  }
-};
-
-#define KG_CUDA(call, what)                              \
-  do {                                                   \
-    cudaError_t e__ = (call);                            \
-    if (e__ != cudaSuccess) return ctx->cuda_fail(e__, what); \
-  } while (0)
+using namespace kgctx;
 
 extern "C" {
 
@@ -185,6 +99,7 @@ void kg_destroy(kg_ctx* ctx) {
     if (ctx->ev_h2d[b]) cudaEventDestroy(ctx->ev_h2d[b]);
     if (ctx->ev_k[b]) cudaEventDestroy(ctx->ev_k[b]);
   }
+  kgctx::free_multi(ctx);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   delete ctx;

@@ -1,0 +1,167 @@
+// ctx.hpp -- the context behind the C ABI (private to the library).
+#pragma once
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/kgwas_cuda.h"
+#include "kernels.hpp"
+#include "prep.hpp"
+
+namespace kgctx {
+
+constexpr int NBUF = 2;  // host-run chunk buffers in flight
+
+template <class T>
+inline void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+// Smallest r2 that can still give p = erfc(sqrt(T/2)) <= p_thresh with
+// T = n log(1/(1-r2)) (src/kgwas.cpp:51-52), lowered by a relative margin of
+// 1e-9 so that k-mers below it are certainly not emitted.  -1 when every
+// tested k-mer may be emitted.
+inline double r2_candidate(double p_thresh, int n) {
+  if (!(p_thresh < 1.0)) return -1.0;
+  if (p_thresh <= 0.0) return 2.0;
+  double lo = 0.0, hi = 1.0;
+  while (std::erfc(std::sqrt(0.5 * hi)) > p_thresh && hi < 1e7) hi *= 2;
+  for (int it = 0; it < 200; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (std::erfc(std::sqrt(0.5 * mid)) > p_thresh) lo = mid; else hi = mid;
+  }
+  const double r2 = -std::expm1(-lo / (double)n);
+  return r2 * (1.0 - 1e-9);
+}
+
+// Epilogue constants of one prepared phenotype.
+inline void fill_epi(kg::EpiParams& P, const kg::Prepared& p, const kg_opts& o, bool refine) {
+  std::memset(&P, 0, sizeof(P));
+  P.n = p.n;
+  P.k = p.k;
+  P.b = p.b;
+  P.kappa = p.kappa;
+  P.yyM = p.yyM;
+  P.ynorm = p.ynorm;
+  P.corr_thr = o.corr_threshold;
+  P.p_thresh = std::pow(10.0, -o.log10_thresh);
+  P.r2_cand = r2_candidate(P.p_thresh, p.n);
+  P.thr2_ynorm2 = o.corr_threshold * o.corr_threshold * p.ynorm * p.ynorm;
+  for (int j = 0; j < p.k; ++j) {
+    P.a[j] = p.a[j];
+    P.g[j] = p.g[j];
+  }
+  if (refine) {
+    P.refine = 1;
+    P.r2_ref = -std::expm1(-kg::REFINE_CHISQ / (double)p.n);
+  }
+}
+
+// State of the many-phenotype path.
+struct Multi {
+  int np = 0, n_row = 0, NP = 0, G = 0, kpad = 0, cm = 0, nsteps = 0;
+  int8_t* dB = nullptr;
+  kg::MPheno* dPh = nullptr;
+  double* dV = nullptr;
+  size_t vstride = 0;
+  unsigned long long* dCounters = nullptr;
+  unsigned long long* dTested = nullptr;
+  size_t tested_cap = 0;
+  kg_phit* dHits = nullptr;
+  unsigned long long hit_cap = 0;
+  unsigned long long* dShard = nullptr;
+  int shard_cap = 0;
+  int n_shards = 1;
+  std::vector<unsigned long long> shard_host;
+  std::vector<kg_phit> hits;
+  std::vector<uint64_t> tested;
+  unsigned long long counters[4] = {0, 0, 0, 0};
+  // launch shape chosen by the autotuner: x tiles resident, B ring stages
+  int xs = 1, nb = 4;
+  bool tuned = false;
+  int tuned_nbox = -1;
+  // pending device launch and its captured graph
+  bool pending = false;
+  const uint64_t* pend_x = nullptr;
+  uint64_t pend_m = 0;
+  uint32_t pend_wpk = 0;
+  cudaStream_t pend_stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  const uint64_t* g_x = nullptr;
+  uint64_t g_m = 0;
+  uint32_t g_wpk = 0;
+  cudaStream_t g_stream = nullptr;
+  int g_seen = 0;
+};
+
+}  // namespace kgctx
+
+struct kg_ctx {
+  kg_opts opts{};
+  int num_sms = 0;
+  cudaStream_t stream = nullptr, copy_stream = nullptr;
+  std::string err;
+  bool have_structure = false;
+  int n_row = 0;  // samples per packed row
+  kg::Prepared prep;
+  kg::LimbCols limbs;
+  kg::EpiParams P{};
+  kg::LimbMap LM{};
+  // structure on the device
+  double* dV = nullptr;
+  int cm = 0, nsteps = 0;
+  int8_t* dB = nullptr;      // B image of the smem-A kernel
+  int8_t* dBts = nullptr;    // B image of the TMEM-A kernel
+  int nchunk = 0;
+  // outputs on the device
+  unsigned long long* dCounters = nullptr;
+  kg_hit* dHits = nullptr;
+  unsigned long long hit_cap = 0;
+  unsigned long long* dCand = nullptr;  // FP64 refinement candidates (split form)
+  unsigned long long cand_cap = 0;
+  uint8_t* dTested = nullptr;
+  double* dStat[7] = {};
+  size_t stat_cap = 0;
+  // host result
+  std::vector<kg_hit> hits;
+  unsigned long long counters[3] = {0, 0, 0};
+  // pending device launch
+  bool pending = false;
+  const uint64_t* pend_x = nullptr;
+  uint64_t pend_m = 0;
+  uint32_t pend_wpk = 0;
+  bool pend_stats = false;
+  cudaStream_t pend_stream = nullptr;
+  int launches = 0;
+  const char* last_kernel = "";
+  // host-run buffers
+  uint64_t* dChunk[kgctx::NBUF] = {};
+  void* hStage[kgctx::NBUF] = {};
+  size_t chunk_bytes = 0;
+  cudaEvent_t ev_h2d[kgctx::NBUF] = {}, ev_k[kgctx::NBUF] = {};
+  // many phenotypes
+  kgctx::Multi mp;
+
+  int fail(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+  int cuda_fail(cudaError_t e, const char* what) {
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return KG_ERR_CUDA;
+  }
+};
+
+#define KG_CUDA(call, what)                                    \
+  do {                                                         \
+    cudaError_t e__ = (call);                                  \
+    if (e__ != cudaSuccess) return ctx->cuda_fail(e__, what);  \
+  } while (0)
+
+namespace kgctx {
+void free_multi(kg_ctx* ctx);  // capi_multi.cpp
+}  // namespace kgctx

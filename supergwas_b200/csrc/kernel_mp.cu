@@ -1,0 +1,594 @@
+// kernel_mp.cu -- many phenotypes per k-mer tile (split precision).
+//
+// The reference tests one phenotype per process and re-reads the batch for
+// each (HPC/kgwas/kgwas_cols.sh:22-65).  Here a persistent CTA per SM takes a
+// 128-k-mer tile, keeps its packed rows resident in shared memory, and runs
+// every phenotype over it:
+//   warps 0-3   epilogue: per phenotype of the group, limb recombination and
+//               the FP64 statistic (src/kgwas.cpp:44-56, 182-218); tested
+//               counts per (shard, phenotype), hit and refinement records;
+//   warps 4-19  unpack, four groups: 128 samples of the resident tile ->
+//               int8 (0 / -128) -> one TMEM A stage (tcgen05.st);
+//   warp 20     x producer: the tile's packed rows, one 2-D TMA load per
+//               1024 samples (128-byte swizzle, no multicast);
+//   warp 21     B producer: the int8 limbs of each phenotype group, one
+//               128-sample x N chunk per bulk copy from L2 into a ring;
+//   warp 22     MMA: tcgen05.mma kind::i8, A from TMEM, B from the ring,
+//               into one of two TMEM accumulators (N = phenotypes per group x
+//               slot width <= 128 columns).
+// Group gi of a tile re-unpacks the tile (cheap: it is on chip) while the
+// previous group's accumulator is drained by the epilogue.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "device.cuh"
+#include "kernels.hpp"
+
+namespace kg {
+
+constexpr int MP_TM = 128;
+constexpr int MP_KS = 128;
+constexpr int MP_UG = 4;
+constexpr int MP_LU = 3, MP_LY = 5;
+constexpr int MP_WARP_UNPACK0 = 4, MP_WARP_XP = 4 + 4 * MP_UG, MP_WARP_BP = MP_WARP_XP + 1,
+              MP_WARP_MMA = MP_WARP_BP + 1;
+constexpr int MP_THREADS = 32 * (MP_WARP_MMA + 1);
+constexpr uint32_t MP_BOXB = MP_TM * 128;  // one TMA box: 128 rows x 128 bytes
+constexpr unsigned long long MP_KMER_MASK = (1ull << 48) - 1;
+
+__host__ __device__ constexpr int mp_a0(int N) { return ((2 * N + 31) / 32) * 32; }
+__host__ __device__ constexpr int mp_ast(int N) { return (512 - mp_a0(N)) / 32 > 16 ? 16 : (512 - mp_a0(N)) / 32; }
+
+struct MpSmem {
+  uint32_t x, b, bars, tmem, abort, total;
+};
+__host__ __device__ inline MpSmem mp_smem(int nbox, int xs, int nb, int N) {
+  MpSmem L;
+  L.x = 0;
+  L.b = (uint32_t)xs * nbox * MP_BOXB;
+  L.bars = L.b + (uint32_t)nb * 128 * N;
+  L.tmem = L.bars + 8 * (2 * 2 + 2 * 8 + 2 * 16 + 4 + 1);
+  L.abort = L.tmem + 8;
+  L.total = L.abort + 8;
+  return L;
+}
+
+__device__ __forceinline__ void mp_tma_2d(uint32_t dst, const void* tmap, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"(tmap), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void mp_st32(uint32_t taddr, const uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+      "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]),
+      "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]),
+      "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
+      : "memory");
+}
+
+__device__ __forceinline__ bool mp_wait(uint32_t bar, uint32_t parity, volatile int* abort,
+                                        unsigned long long* counters, unsigned code) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = gtimer_ns();
+  for (;;) {
+    if (mbar_try(bar, parity)) return true;
+    if (*abort) return false;
+    if (gtimer_ns() - t0 > WAIT_LIMIT_NS) {
+      atomicOr(counters + 2, (unsigned long long)code);
+      *abort = 1;
+      return false;
+    }
+  }
+}
+
+// Shard of a global k-mer index (shard_start ascending, shard_start[0] = 0).
+__device__ __forceinline__ int mp_shard(const DevOutMP& O, unsigned long long gk) {
+  int lo = 0, hi = O.n_shards - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (O.shard_start[mid] <= gk) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Statistic of one (k-mer, phenotype) from the exact integer sums, as the
+// division-free screen of finish_kmer_fast; writes the outcome flags.
+__device__ __forceinline__ void mp_eval(const EpiParams& P, bool valid, int c, double ss, double gs, double ey,
+                                        bool& tested, bool& hit, bool& cand, double& T, double& p, double& effect) {
+  const int n = P.n;
+  tested = valid && c > 0 && c < n && !(P.ynorm < 1e-12);
+  if (tested && P.corr_thr > 0.0) {
+    const double xcn2 = (double)c * (double)(n - c) / (double)n;
+    const double xyc = ey + gs + P.kappa * (double)c;
+    tested = xyc * xyc >= P.thr2_ynorm2 * xcn2;
+  }
+  hit = cand = false;
+  T = 0;
+  p = 1;
+  effect = 0;
+  if (!tested) return;
+  const double xxM = (double)c - ss, xyM = P.b * (double)c + ey;
+  const double eps = 1e-12;
+  if (!(xxM > eps && P.yyM > eps)) {
+    hit = p <= P.p_thresh;
+    return;
+  }
+  const double q = xyM * xyM, den = xxM * P.yyM;
+  if (P.refine && q >= P.r2_ref * den) {
+    cand = true;
+  } else if (q >= P.r2_cand * den) {
+    double r2 = q / den;
+    if (r2 < 0) r2 = 0;
+    if (r2 >= 1) r2 = 1 - 1e-15;
+    T = (double)n * log(1.0 / (1.0 - r2));
+    p = erfc(sqrt(0.5 * T));
+    effect = xyM / den;
+    hit = p <= P.p_thresh;
+  }
+}
+
+template <int NP>
+__global__ void __launch_bounds__(MP_THREADS, 1)
+    mp_kernel(const __grid_constant__ CUtensorMap tmap, unsigned long long m, int nbox, int nchunk, int G,
+              int xs_slots, int nb, const int8_t* __restrict__ Bimg, const MPheno* __restrict__ ph,
+              const DevOutMP O) {
+  constexpr int PPG = 128 / NP;
+  constexpr int N = PPG * NP;
+  constexpr int A0 = mp_a0(N);
+  constexpr int AST = mp_ast(N);
+  constexpr uint32_t IDESC = idesc_i8(MP_TM, N);
+  constexpr uint32_t BCH = 128u * N;  // bytes of one B chunk (128 samples x N)
+  constexpr int KU_MAX = (NP - 1 - MP_LY) / MP_LU;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t* gbase = smem_raw + (base - raw);
+  const MpSmem L = mp_smem(nbox, xs_slots, nb, N);
+  const uint32_t sx = base + L.x, sb = base + L.b;
+  const uint32_t x_full = base + L.bars, x_empty = x_full + 16;
+  const uint32_t b_full = x_empty + 16, b_empty = b_full + 64;
+  const uint32_t a_full = b_empty + 64, a_empty = a_full + 128;
+  const uint32_t acc_full = a_empty + 128, acc_empty = acc_full + 16, drain = acc_empty + 16;
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(gbase + L.tmem);
+  volatile int* s_abort = reinterpret_cast<volatile int*>(gbase + L.abort);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t xslot = (uint32_t)nbox * MP_BOXB;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(s_tmem))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 32) {
+    for (int s = 0; s < xs_slots; ++s) {
+      mbar_init(x_full + 8 * s, 1);
+      mbar_init(x_empty + 8 * s, 4 * MP_UG);
+    }
+    for (int s = 0; s < nb; ++s) {
+      mbar_init(b_full + 8 * s, 1);
+      mbar_init(b_empty + 8 * s, 1);
+    }
+    for (int t = 0; t < AST; ++t) {
+      mbar_init(a_full + 8 * t, 4);
+      mbar_init(a_empty + 8 * t, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(acc_full + 8 * b, 1);
+      mbar_init(acc_empty + 8 * b, 4);
+    }
+    mbar_init(drain, 1);
+    *s_abort = 0;
+    mbar_fence_init();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+  const unsigned long long ntiles = (m + MP_TM - 1) / MP_TM;
+
+  if (warp == MP_WARP_XP) {
+    // ---------------------------------------------------------- x producer
+    if (lane == 0) {
+      asm volatile("prefetch.tensormap [%0];" ::"l"(&tmap) : "memory");
+      uint32_t last_use[2] = {0xffffffffu, 0xffffffffu};
+      uint32_t it = 0;
+      for (unsigned long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        const uint32_t xs = it % xs_slots, u = it / xs_slots;
+        if (u > 0 && !mp_wait(x_empty + 8 * xs, (u - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_FULL)) break;
+        mbar_arrive_expect_tx(x_full + 8 * xs, xslot);
+        for (int bx = 0; bx < nbox; ++bx)
+          mp_tma_2d(sx + xs * xslot + bx * MP_BOXB, &tmap, bx * 128, (int)(tile * MP_TM), x_full + 8 * xs);
+        last_use[xs] = u;
+      }
+      for (int s = 0; s < xs_slots; ++s)
+        if (last_use[s] != 0xffffffffu) mbar_wait(x_full + 8 * s, last_use[s] & 1, O.counters, ERR_TIMEOUT_FULL);
+    }
+  } else if (warp == MP_WARP_BP) {
+    // ---------------------------------------------------------- B producer
+    if (lane == 0) {
+      uint32_t last_use[8];
+      for (int s = 0; s < 8; ++s) last_use[s] = 0xffffffffu;
+      uint32_t h = 0;
+      bool ok = true;
+      for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x)
+        for (int gi = 0; gi < G && ok; ++gi)
+          for (int kc = 0; kc < nchunk; ++kc, ++h) {
+            const uint32_t s = h % nb, u = h / nb;
+            if (u > 0 && !mp_wait(b_empty + 8 * s, (u - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_FULL)) {
+              ok = false;
+              break;
+            }
+            mbar_arrive_expect_tx(b_full + 8 * s, BCH);
+            bulk_g2s(sb + s * BCH, Bimg + ((size_t)gi * nchunk + kc) * BCH, BCH, b_full + 8 * s);
+            last_use[s] = u;
+          }
+      for (int s = 0; s < nb; ++s)
+        if (last_use[s] != 0xffffffffu) mbar_wait(b_full + 8 * s, last_use[s] & 1, O.counters, ERR_TIMEOUT_FULL);
+    }
+  } else if (warp == MP_WARP_MMA) {
+    // ----------------------------------------------------------------- MMA
+    if (lane == 0) {
+      uint32_t g = 0, h = 0, w = 0;
+      bool ok = true;
+      for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        for (int gi = 0; gi < G && ok; ++gi, ++w) {
+          const uint32_t b = w & 1, v = w >> 1;
+          if (v > 0 && !mp_wait(acc_empty + 8 * b, (v - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          for (int kc = 0; kc < nchunk; ++kc, ++g, ++h) {
+            const uint32_t t = g % AST, s = h % nb;
+            if (!mp_wait(a_full + 8 * t, (g / AST) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA) ||
+                !mp_wait(b_full + 8 * s, (h / nb) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+#pragma unroll
+            for (int ks = 0; ks < MP_KS / 32; ++ks) {
+              const uint64_t bd = sdesc_noswz(sb + s * BCH + ks * 2 * (N * 16), N * 16, 128);
+              tc_mma_i8_ts(tmem + b * N, tmem + A0 + t * 32 + ks * 8, bd, IDESC, (kc | ks) != 0);
+            }
+            tc_commit(a_empty + 8 * t);
+            tc_commit(b_empty + 8 * s);
+          }
+          if (ok) tc_commit(acc_full + 8 * b);
+        }
+      }
+      tc_commit(drain);
+      mbar_wait(drain, 0, O.counters, ERR_TIMEOUT_MMA);
+    }
+  } else if (warp >= MP_WARP_UNPACK0) {
+    // -------------------------------------------------------------- unpack
+    const int grp = (warp - MP_WARP_UNPACK0) >> 2;
+    const int q = warp & 3;
+    const int r = q * 32 + lane;
+    const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+    uint32_t g = 0, it = 0;
+    bool ok = true;
+    for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
+      const uint32_t xs = it % xs_slots;
+      if (!__all_sync(0xffffffffu, mp_wait(x_full + 8 * xs, (it / xs_slots) & 1, s_abort, O.counters,
+                                           ERR_TIMEOUT_FULL)))
+        break;
+      const uint32_t tb = sx + xs * xslot;
+      for (int gi = 0; gi < G && ok; ++gi) {
+        for (int kc = 0; kc < nchunk; ++kc, ++g) {
+          if ((int)(g % MP_UG) != grp) continue;
+          const uint32_t t = g % AST, u = g / AST;
+          if (u > 0 && !__all_sync(0xffffffffu, mp_wait(a_empty + 8 * t, (u - 1) & 1, s_abort, O.counters,
+                                                         ERR_TIMEOUT_MMA))) {
+            ok = false;
+            break;
+          }
+          const int bx = kc >> 3, c = kc & 7;
+          uint4 v;
+          asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];"
+                       : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                       : "r"(tb + bx * MP_BOXB + r * 128 + ((c ^ (r & 7)) << 4)));
+          const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
+          uint32_t o[32];
+#pragma unroll
+          for (int qq = 0; qq < 4; ++qq)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) o[qq * 8 + j] = (w4[qq] * (1u << (7 - j))) & 0x80808080u;
+          mp_st32(tmem + lane_base + A0 + t * 32, o);
+          tc_wait_st();
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(a_full + 8 * t);
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(x_empty + 8 * xs);
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int q = warp & 3;
+    const int r = q * 32 + lane;
+    const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+    uint32_t w = 0;
+    bool ok = true;
+    for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+      const unsigned long long local = tile * MP_TM + r;
+      const bool valid = local < m;
+      const unsigned long long gk = O.kmer_offset + local;
+      const int shard = mp_shard(O, gk);
+      const unsigned match = __match_any_sync(0xffffffffu, shard);
+      const bool leader = lane == __ffs(match) - 1;
+      for (int gi = 0; gi < G; ++gi, ++w) {
+        const uint32_t b = w & 1, v = w >> 1;
+        if (!__all_sync(0xffffffffu, mp_wait(acc_full + 8 * b, v & 1, s_abort, O.counters, ERR_TIMEOUT_MMA))) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        for (int pp = 0; pp < PPG; ++pp) {
+          const int p = gi * PPG + pp;
+          if (p >= O.n_pheno) break;
+          // this phenotype's slot of the accumulator: NP int32 columns
+          uint32_t d[NP];
+#pragma unroll
+          for (int c16 = 0; c16 < NP / 16; ++c16) {
+            uint32_t rr[16];
+            tc_ld16(tmem + lane_base + b * N + pp * NP + c16 * 16, rr);
+#pragma unroll
+            for (int e = 0; e < 16; ++e) d[c16 * 16 + e] = rr[e];
+          }
+          tc_wait_ld();
+          const MPheno& ME = ph[p];
+          const int k = ME.P.k;
+          const int drop0 = ME.drop0;
+          const int c = (-(int)d[0]) >> 7;
+          double vy = (double)((-(int)d[1]) >> 7);
+#pragma unroll
+          for (int l = 1; l < MP_LY; ++l) vy = fma(vy, 256.0, (double)((-(int)d[1 + l]) >> 7));
+          const double ey = vy * ME.LM.scale[k];
+          double ss = 0, gs = 0;
+          if (drop0) {
+            const double s0 = ME.P.a[0] * (double)c;
+            ss = s0 * s0;
+          }
+#pragma unroll
+          for (int jj = 0; jj < KU_MAX; ++jj) {
+            const int j = jj + drop0;
+            if (j < k) {
+              const int o = 1 + MP_LY + MP_LU * jj;
+              double vj = (double)((-(int)d[o]) >> 7);
+#pragma unroll
+              for (int l = 1; l < MP_LU; ++l) vj = fma(vj, 256.0, (double)((-(int)d[o + l]) >> 7));
+              const double e = vj * ME.LM.scale[j];
+              const double sj = fma(ME.P.a[j], (double)c, e);
+              ss = fma(sj, sj, ss);
+              gs = fma(ME.P.g[j], e, gs);
+            }
+          }
+          bool tested, hit, cand;
+          double T, pv, effect;
+          mp_eval(ME.P, valid, c, ss, gs, ey, tested, hit, cand, T, pv, effect);
+          // tested count of (shard, phenotype): one atomic per shard present in the warp
+          const unsigned tm = __ballot_sync(0xffffffffu, tested);
+          if (leader && (tm & match))
+            atomicAdd(O.tested + (size_t)shard * O.n_pheno + p, (unsigned long long)__popc(tm & match));
+          const unsigned hm = __ballot_sync(0xffffffffu, hit);
+          if (hm) {
+            unsigned long long hb = 0;
+            const int hl = __ffs(hm) - 1;
+            if (lane == hl) hb = atomicAdd(O.counters + 1, (unsigned long long)__popc(hm));
+            hb = __shfl_sync(0xffffffffu, hb, hl);
+            if (hit) {
+              const unsigned long long slot = hb + __popc(hm & ((1u << lane) - 1u));
+              if (slot < O.hit_cap) {
+                kg_phit hrec;
+                hrec.kmer = gk;
+                hrec.pheno = p;
+                hrec.shard = shard;
+                hrec.effect = effect;
+                hrec.pval = pv;
+                hrec.chisq = T;
+                O.hits[slot] = hrec;
+              } else {
+                atomicOr(O.counters + 2, (unsigned long long)ERR_HIT_OVERFLOW);
+              }
+            }
+          }
+          const unsigned cm = __ballot_sync(0xffffffffu, cand);
+          if (cm) {
+            unsigned long long cb = 0;
+            const int cl = __ffs(cm) - 1;
+            if (lane == cl) cb = atomicAdd(O.counters + 3, (unsigned long long)__popc(cm));
+            cb = __shfl_sync(0xffffffffu, cb, cl);
+            if (cand) {
+              const unsigned long long slot = cb + __popc(cm & ((1u << lane) - 1u));
+              if (slot < O.cand_cap) O.cand[slot] = gk | ((unsigned long long)p << 48);
+              else atomicOr(O.counters + 2, (unsigned long long)ERR_CAND_OVERFLOW);
+            }
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acc_empty + 8 * b);
+      }
+    }
+  }
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+}
+
+// FP64 recomputation of the candidates of a multi-phenotype launch: one
+// warp per (k-mer, phenotype), the phenotype's FP64 columns at V + p*vstride.
+template <int CM>
+__global__ void __launch_bounds__(256) mp_refine_kernel(const uint64_t* __restrict__ x, int wpk,
+                                                        const double* __restrict__ V, int vrows,
+                                                        unsigned long long vstride, const MPheno* __restrict__ ph,
+                                                        const DevOutMP O) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x >> 5);
+  unsigned long long ncand = O.counters[3];
+  if (ncand > O.cand_cap) ncand = O.cand_cap;
+  for (unsigned long long w = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < ncand;
+       w += warps) {
+    const unsigned long long ent = O.cand[w];
+    const unsigned long long gk = ent & MP_KMER_MASK;
+    const int p = (int)(ent >> 48);
+    const EpiParams& P = ph[p].P;
+    const double* Vp = V + (size_t)p * vstride;
+    const uint64_t* row = x + (gk - O.kmer_offset) * (unsigned long long)wpk;
+    double acc[CM];
+#pragma unroll
+    for (int j = 0; j < CM; ++j) acc[j] = 0.0;
+    for (int wi = lane; wi < wpk; wi += 32) {
+      uint64_t bits = __ldg(row + wi);
+      while (bits) {
+        const int b = __ffsll((long long)bits) - 1;
+        bits &= bits - 1;
+        const int smp = wi * 64 + b;
+        if (smp < vrows) {
+          const double* vv = Vp + (size_t)smp * CM;
+#pragma unroll
+          for (int j = 0; j < CM; ++j) acc[j] += vv[j];
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < CM; ++j)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+    if (lane == 0) {
+      const int c = (int)acc[0];
+      double ss = 0, ey = 0;
+#pragma unroll
+      for (int j = 1; j < CM; ++j) {
+        if (j <= P.k) {
+          const double sj = P.a[j - 1] * (double)c + acc[j];
+          ss += sj * sj;
+        } else if (j == P.k + 1) {
+          ey = acc[j];
+        }
+      }
+      const double xxM = (double)c - ss, xyM = P.b * (double)c + ey;
+      double effect = 0, T = 0, pv = 1;
+      if (xxM > 1e-12 && P.yyM > 1e-12) {
+        double r2 = (xyM * xyM) / (xxM * P.yyM);
+        if (r2 < 0) r2 = 0;
+        if (r2 >= 1) r2 = 1 - 1e-15;
+        T = (double)P.n * log(1.0 / (1.0 - r2));
+        pv = erfc(sqrt(0.5 * T));
+        effect = xyM / (xxM * P.yyM);
+      }
+      if (pv <= P.p_thresh) {
+        const unsigned long long slot = atomicAdd(O.counters + 1, 1ull);
+        if (slot < O.hit_cap) {
+          kg_phit h;
+          h.kmer = gk;
+          h.pheno = p;
+          h.shard = mp_shard(O, gk);
+          h.effect = effect;
+          h.pval = pv;
+          h.chisq = T;
+          O.hits[slot] = h;
+        } else {
+          atomicOr(O.counters + 2, (unsigned long long)ERR_HIT_OVERFLOW);
+        }
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------- host
+
+static PFN_cuTensorMapEncodeTiled_v12000 mp_encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+size_t mp_smem_bytes(int nbox, int xs, int nb, int N) { return mp_smem(nbox, xs, nb, N).total + 1024; }
+
+bool mp_supported(int NP, int wpk) {
+  if (NP < 16 || NP > 128 || NP % 16) return false;
+  if (wpk * 8 < 128) return false;
+  return mp_encode_fn() != nullptr;
+}
+
+template <int NP>
+static cudaError_t launch_mp_t(const LaunchMp& L, const CUtensorMap& tm, cudaStream_t st) {
+  constexpr int N = (128 / NP) * NP;
+  const int nbox = (L.wpk * 8 + 127) / 128;
+  const size_t smem = mp_smem_bytes(nbox, L.xs, L.nb, N);
+  cudaError_t e = cudaFuncSetAttribute(mp_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const unsigned long long tiles = (L.m + MP_TM - 1) / MP_TM;
+  unsigned long long grid = (unsigned long long)L.num_sms;
+  if (grid > tiles) grid = tiles;
+  mp_kernel<NP><<<(unsigned)grid, MP_THREADS, smem, st>>>(tm, L.m, nbox, L.kpad / MP_KS, L.G, L.xs, L.nb, L.Bimg,
+                                                          L.ph, *L.O);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mp(const LaunchMp& L, cudaStream_t st) {
+  auto enc = mp_encode_fn();
+  if (!enc) return cudaErrorNotSupported;
+  CUtensorMap tm;
+  const cuuint64_t rowbytes = (cuuint64_t)L.wpk * 8;
+  cuuint64_t gdim[2] = {rowbytes, (cuuint64_t)L.m};
+  cuuint64_t gstride[1] = {rowbytes};
+  cuuint32_t box[2] = {128, MP_TM};
+  cuuint32_t estr[2] = {1, 1};
+  if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)L.x, gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return cudaErrorInvalidValue;
+  switch (L.NP) {
+    case 16: return launch_mp_t<16>(L, tm, st);
+    case 32: return launch_mp_t<32>(L, tm, st);
+    case 48: return launch_mp_t<48>(L, tm, st);
+    case 64: return launch_mp_t<64>(L, tm, st);
+    case 80: return launch_mp_t<80>(L, tm, st);
+    case 96: return launch_mp_t<96>(L, tm, st);
+    case 112: return launch_mp_t<112>(L, tm, st);
+    case 128: return launch_mp_t<128>(L, tm, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int CM>
+static cudaError_t launch_mp_refine_t(const LaunchMpRefine& L, cudaStream_t st) {
+  mp_refine_kernel<CM><<<(unsigned)(L.num_sms * 4), 256, 0, st>>>(L.x, L.wpk, L.V, L.vrows, L.vstride, L.ph, *L.O);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mp_refine(const LaunchMpRefine& L, cudaStream_t st) {
+  switch (L.cm) {
+    case 8: return launch_mp_refine_t<8>(L, st);
+    case 12: return launch_mp_refine_t<12>(L, st);
+    case 16: return launch_mp_refine_t<16>(L, st);
+    case 20: return launch_mp_refine_t<20>(L, st);
+    case 24: return launch_mp_refine_t<24>(L, st);
+    case 28: return launch_mp_refine_t<28>(L, st);
+    case 36: return launch_mp_refine_t<36>(L, st);
+    case 44: return launch_mp_refine_t<44>(L, st);
+    case 52: return launch_mp_refine_t<52>(L, st);
+    case 68: return launch_mp_refine_t<68>(L, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace kg

@@ -1,25 +1,29 @@
 // kernel_ts.cu -- split-precision association kernel with the unpacked x
 // operand held in tensor memory.
 //
-// One persistent CTA per SM, warp-specialised (704 threads):
+// One persistent CTA per SM, warp-specialised (448 threads):
 //   warps 0-3   epilogue: tcgen05.ld of the int32 accumulators (one TMEM lane
 //               = one k-mer), limb recombination, FP64 statistics,
 //               warp-aggregated hit compaction;
-//   warps 4-19  unpack, four groups of four (one warp per TMEM lane quarter),
-//               the groups taking K stages in turn so that four stores to
+//   warps 4-11  unpack, two groups of four (one warp per TMEM lane quarter),
+//               the groups taking K stages in turn so that two stores to
 //               tensor memory are in flight per lane quarter:
 //               read 128 samples of a packed row from the TMA-filled shared
 //               tile and write them as int8 (0 / -128) straight into a TMEM
 //               A stage with tcgen05.st -- the unpacked operand never touches
 //               shared memory;
-//   warp 20     producer: one 2-D TMA load (128 rows x 128 bytes, 128-byte
+//   warp 12     producer: one 2-D TMA load (128 rows x 128 bytes, 128-byte
 //               swizzle, no multicast) per 1024 samples of a 128-k-mer tile;
-//   warp 21     MMA: tcgen05.mma kind::i8, A from TMEM, B (the int8 limbs of
+//   warp 13     MMA: tcgen05.mma kind::i8, A from TMEM, B (the int8 limbs of
 //               the centred structure and phenotype columns, resident in
 //               shared memory for the whole launch) from a smem descriptor,
 //               accumulating into one of two TMEM accumulators.
 // Tile = 128 k-mers (M), K stage = 128 samples (32 TMEM columns), N = 16..128.
-// TMEM (512 columns): accumulators at [0, 2N), A stages after them.
+// TMEM (512 columns): NBUF accumulator buffers of S split-K accumulators of
+// N columns each, then the A stages.  K stage kc accumulates into split
+// kc % S, so S independent MMA chains are in flight instead of one serial
+// chain of K/32 dependent accumulations; the epilogue adds the S int32
+// partial sums (exact).
 //
 // The accumulators hold -128 * sum_i x_i * digit_l(i) for every limb l; the
 // epilogue recombines the limbs exactly in int64, scales by 2^-s / 128, and
@@ -28,6 +32,7 @@
 #include <cudaTypedefs.h>
 
 #include <cstdio>
+#include <cstdlib>
 
 #include "device.cuh"
 #include "kernels.hpp"
@@ -38,15 +43,15 @@ constexpr int TS_TM = 128;
 constexpr int TS_KS = 128;         // samples per A stage
 constexpr int TS_BOX = 1024;       // samples per TMA box (128 bytes)
 constexpr int TS_XST = 4;          // packed boxes in flight
-constexpr int TS_UG = 4;           // unpack groups
+constexpr int TS_UG = 2;           // unpack groups
 constexpr int TS_THREADS = 32 * (4 + 4 * TS_UG + 2);
 constexpr int TS_LU = 3, TS_LY = 5;
 constexpr uint32_t TS_XBYTES = TS_TM * 128;  // one box: 128 rows x 128 bytes
 constexpr int TS_WARP_UNPACK0 = 4, TS_WARP_PROD = 4 + 4 * TS_UG, TS_WARP_MMA = TS_WARP_PROD + 1;
 
-__host__ __device__ constexpr int ts_a0(int N) { return ((2 * N + 31) / 32) * 32; }
-__host__ __device__ constexpr int ts_ast(int N) {
-  return (512 - ts_a0(N)) / 32 > 16 ? 16 : (512 - ts_a0(N)) / 32;
+__host__ __device__ constexpr int ts_a0(int N, int S, int NB) { return ((NB * S * N + 31) / 32) * 32; }
+__host__ __device__ constexpr int ts_ast(int N, int S, int NB) {
+  return (512 - ts_a0(N, S, NB)) / 32 > 16 ? 16 : (512 - ts_a0(N, S, NB)) / 32;
 }
 
 struct TsSmem {  // offsets from the 1024-aligned base
@@ -101,10 +106,10 @@ __device__ __forceinline__ bool ts_wait(uint32_t bar, uint32_t parity, volatile 
 template <int N, bool DROP0>
 __global__ void __launch_bounds__(TS_THREADS, 1)
     ts_kernel(const __grid_constant__ CUtensorMap tmap, unsigned long long m, int nbox, int nchunk,
-              const int8_t* __restrict__ Bimg, int b_bytes, const __grid_constant__ EpiParams P,
+              const int8_t* __restrict__ Bimg, int b_bytes, int S, int NB, const __grid_constant__ EpiParams P,
               const __grid_constant__ LimbMap LM, const DevOut O) {
-  constexpr int A0 = ts_a0(N);
-  constexpr int AST = ts_ast(N);
+  const int A0 = ts_a0(N, S, NB);
+  const int AST = ts_ast(N, S, NB);
   constexpr uint32_t IDESC = idesc_i8(TS_TM, N);
   constexpr int KU_MAX = (N - 1 - TS_LY) / TS_LU;  // U columns that fit in N
   extern __shared__ uint8_t smem_raw[];
@@ -135,7 +140,7 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
       mbar_init(a_full + 8 * t, 4);   // the 4 warps of one unpack group
       mbar_init(a_empty + 8 * t, 1);  // tcgen05.commit
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < NB; ++b) {
       mbar_init(acc_full + 8 * b, 1);
       mbar_init(acc_empty + 8 * b, 4);
     }
@@ -186,7 +191,7 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
       bool ok = ts_wait(b_full, 0, s_abort, O.counters, ERR_TIMEOUT_FULL);
       uint32_t g = 0, i = 0;
       for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++i) {
-        const uint32_t b = i & 1, v = i >> 1;
+        const uint32_t b = i % NB, v = i / NB;
         if (v > 0 && !ts_wait(acc_empty + 8 * b, (v - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA)) {
           ok = false;
           break;
@@ -199,11 +204,12 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
             break;
           }
           tc_fence_after();
+          const uint32_t d_t = tmem + (b * S + kc % S) * N;  // split-K accumulator of this stage
 #pragma unroll
           for (int ks = 0; ks < TS_KS / 32; ++ks) {
             const uint32_t a_t = tmem + A0 + t * 32 + ks * 8;
             const uint64_t bd = sdesc_noswz(sb + ((kc * TS_KS + ks * 32) / 16) * (N * 16), N * 16, 128);
-            tc_mma_i8_ts(tmem + b * N, a_t, bd, IDESC, (kc | ks) != 0);
+            tc_mma_i8_ts(d_t, a_t, bd, IDESC, (kc >= S || ks != 0) ? 1u : 0u);
           }
           tc_commit(a_empty + 8 * t);
         }
@@ -271,19 +277,28 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     const int r = q * 32 + lane;
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
     uint32_t i = 0;
+    const int nsplit = nchunk < S ? nchunk : S;  // splits that received a stage
     for (unsigned long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
-      const uint32_t b = i & 1, v = i >> 1;
+      const uint32_t b = i % NB, v = i / NB;
       if (!__all_sync(0xffffffffu, ts_wait(acc_full + 8 * b, v & 1, s_abort, O.counters, ERR_TIMEOUT_MMA))) break;
       tc_fence_after();
+      // sum the split-K partial accumulators, 16 columns at a time; every
+      // tcgen05.ld completes (wait::ld) before its registers are used
       uint32_t d[N];
 #pragma unroll
       for (int c16 = 0; c16 < N / 16; ++c16) {
         uint32_t rr[16];
-        tc_ld16(tmem + lane_base + b * N + c16 * 16, rr);
+        tc_ld16(tmem + lane_base + b * S * N + c16 * 16, rr);
+        tc_wait_ld();
 #pragma unroll
         for (int e = 0; e < 16; ++e) d[c16 * 16 + e] = rr[e];
+        for (int sp = 1; sp < nsplit; ++sp) {
+          tc_ld16(tmem + lane_base + (b * S + sp) * N + c16 * 16, rr);
+          tc_wait_ld();
+#pragma unroll
+          for (int e = 0; e < 16; ++e) d[c16 * 16 + e] += rr[e];
+        }
       }
-      tc_wait_ld();
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(acc_empty + 8 * b);
@@ -340,10 +355,25 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
+// Split-K accumulators and accumulator buffers for width N (KG_TS_SPLIT=
+// "S,NB" overrides): as many independent chains as fit beside 8 A stages.
+static void ts_shape(int N, int& S, int& NB) {
+  S = N <= 32 ? 4 : N <= 64 ? 4 : 2;
+  NB = N <= 32 ? 2 : 1;
+  if (const char* v = std::getenv("KG_TS_SPLIT")) {
+    int s = 0, b = 0;
+    if (std::sscanf(v, "%d,%d", &s, &b) == 2 && s >= 1 && s <= 8 && b >= 1 && b <= 2 &&
+        ts_ast(N, s, b) >= 4)
+      S = s, NB = b;
+  }
+}
+
 bool ts_supported(int N, int limbs_u, int limbs_y, int kpad, int wpk) {
   if (limbs_u != TS_LU || limbs_y != TS_LY) return false;
   if (N < 16 || N > 128 || N % 16) return false;
-  if (ts_ast(N) < 4) return false;
+  int S, NB;
+  ts_shape(N, S, NB);
+  if (ts_ast(N, S, NB) < 4) return false;
   if ((size_t)kpad * N > 128 * 1024) return false;  // B stays resident in shared memory
   if (wpk * 8 < 128) return false;                   // one TMA box row is 128 bytes
   return encode_fn() != nullptr;
@@ -360,8 +390,10 @@ static cudaError_t launch_ts_t(const LaunchTs& L, const CUtensorMap& tm, cudaStr
   if (grid > tiles) grid = tiles;
   const int nbox = (L.wpk * 8 + 127) / 128;
   const int nchunk = L.kpad / TS_KS;
-  ts_kernel<N, D0><<<(unsigned)grid, TS_THREADS, smem, st>>>(tm, L.m, nbox, nchunk, L.Bimg, b_bytes, *L.P,
-                                                             *L.LM, *L.O);
+  int S, NB;
+  ts_shape(N, S, NB);
+  ts_kernel<N, D0><<<(unsigned)grid, TS_THREADS, smem, st>>>(tm, L.m, nbox, nchunk, L.Bimg, b_bytes, S, NB,
+                                                             *L.P, *L.LM, *L.O);
   return cudaGetLastError();
 }
 

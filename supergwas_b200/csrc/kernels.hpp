@@ -52,6 +52,34 @@ struct LaunchTs {
 bool ts_supported(int N, int limbs_u, int limbs_y, int kpad, int wpk);
 cudaError_t launch_ts(const LaunchTs& L, cudaStream_t st);
 
+struct LaunchMp {
+  const uint64_t* x;          // packed rows (device), 16-byte aligned
+  unsigned long long m;
+  int wpk;
+  int kpad;                   // samples per phenotype group image (multiple of 128)
+  int NP;                     // columns per phenotype slot (multiple of 16, <= 128)
+  int G;                      // phenotype groups (128 / NP phenotypes each)
+  int xs, nb;                 // resident x tiles (1-2), B ring stages (2-8)
+  const int8_t* Bimg;         // G x (kpad/128) chunks of 128 x N bytes (device)
+  const MPheno* ph;           // per-phenotype constants (device)
+  const DevOutMP* O;
+  int num_sms;
+};
+struct LaunchMpRefine {
+  const uint64_t* x;
+  int wpk;
+  const double* V;            // n_pheno blocks of vrows x cm FP64 (device)
+  int vrows, cm;
+  unsigned long long vstride;
+  const MPheno* ph;
+  const DevOutMP* O;
+  int num_sms;
+};
+bool mp_supported(int NP, int wpk);
+size_t mp_smem_bytes(int nbox, int xs, int nb, int N);
+cudaError_t launch_mp(const LaunchMp& L, cudaStream_t st);
+cudaError_t launch_mp_refine(const LaunchMpRefine& L, cudaStream_t st);
+
 int tc_kc();                  // samples per K chunk of the tensor-core kernel
 bool tc_supported_n(int N);
 cudaError_t launch_tc(const LaunchTc& L, cudaStream_t st);

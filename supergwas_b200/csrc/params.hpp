@@ -48,4 +48,26 @@ enum : unsigned { ERR_TIMEOUT_FULL = 1u, ERR_TIMEOUT_MMA = 2u, ERR_HIT_OVERFLOW 
 // absolute 1e-6 bound needs FP64 accuracy; below it 24-bit U limbs suffice.
 constexpr double REFINE_CHISQ = 12.0;
 
+// One phenotype of a multi-phenotype launch (device memory).
+struct MPheno {
+  EpiParams P;
+  LimbMap LM;       // limb columns relative to the phenotype's slot in its group
+  int drop0;        // U column 0 carries no limbs (intercept handled in FP64)
+  int pad;
+};
+
+// Outputs of a multi-phenotype launch.
+struct DevOutMP {
+  unsigned long long* counters;      // [1] hits, [2] error bits, [3] refinement candidates
+  unsigned long long* tested;        // [shard * n_pheno + pheno]
+  kg_phit* hits;
+  unsigned long long hit_cap;
+  unsigned long long* cand;          // kmer | pheno << 48
+  unsigned long long cand_cap;
+  const unsigned long long* shard_start;  // ascending, global k-mer indices
+  int n_shards;
+  int n_pheno;
+  unsigned long long kmer_offset;
+};
+
 }  // namespace kg

@@ -33,14 +33,22 @@ def main():
     g = api.Kgwas(precision="fp64" if a.kernel == "fp64" else "split", corr_threshold=0.0, log10_thresh=6.0)
     g.set_structure(U, y, keep, a.n)
     st = torch.cuda.current_stream()
+    g.launch_device(X.data_ptr(), a.kmers, wpk, st.cuda_stream)  # warm-up
+    g.fetch()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    times = []
     for _ in range(a.launches):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
         g.launch_device(X.data_ptr(), a.kmers, wpk, st.cuda_stream)
+        e1.record(st)
         r = g.fetch()
-    dt = (time.perf_counter() - t0) / a.launches
+        times.append(e0.elapsed_time(e1))
+    times.sort()
+    med = times[len(times) // 2]
     print(f"kernel={g.last_kernel()} kmers={a.kmers} tested={r.n_tested} hits={r.hits.shape[0]} "
-          f"wall_ms_per_launch={dt * 1e3:.3f}")
+          f"device_ms_per_launch={med:.3f} kmers_per_s={a.kmers / med * 1e3:.4g} "
+          f"split={os.environ.get('KG_TS_SPLIT', 'default')}")
     g.close()
 
 

@@ -69,3 +69,52 @@ def structure_and_phenotype(packed_dev: torch.Tensor, n: int, r: int, n_causal: 
     pc1 = Ph[:, -1] if Ph.shape[1] else 0.0
     y = g + 0.5 * pc1 + rng.standard_normal(keep.shape[0])
     return U, y, keep, causal
+
+
+def batched_phenotypes(packed_dev: torch.Tensor, n: int, n_pheno: int, r: int, seed: int,
+                       missing_max: float = 0.3, structure_kmers: int = 20_000, n_causal: int = 50):
+    """Phenotypes for one batch, each with its own missing samples.
+
+    Phenotype p drops a uniform(0, missing_max) fraction of the n samples, and
+    gets its own U (intercept + top r z-scored PCs of a centred k-mer sample
+    restricted to its overlap, as synth.structure_basis) and its own
+    y = causal effects + 0.5 PC1 + N(0, 1).  Returns [(U, y, keep)].
+    """
+    rng = np.random.default_rng(seed)
+    m = packed_dev.shape[0]
+    dev = packed_dev.device
+    sk = min(structure_kmers, m)
+    sidx = np.sort(rng.choice(m, size=sk, replace=False))
+    rows = packed_dev[torch.as_tensor(sidx, device=dev)].cpu().numpy().view(np.uint64)
+    Xs_all = torch.as_tensor(synth.unpack_rows(rows, n), device=dev, dtype=torch.float64)  # (sk, n)
+    out = []
+    for p in range(n_pheno):
+        miss = rng.uniform(0.0, missing_max)
+        keep = np.sort(rng.choice(n, size=n - int(round(miss * n)), replace=False))
+        X = Xs_all[:, torch.as_tensor(keep, device=dev)].T  # (n_p, sk)
+        X = X - X.mean(dim=0, keepdim=True)
+        evals, evecs = torch.linalg.eigh(X @ X.T)
+        Ph = (evecs[:, -r:] * torch.sqrt(torch.clamp(evals[-r:], min=0.0))).cpu().numpy()
+        Ph = Ph - Ph.mean(axis=0, keepdims=True)
+        sd = np.sqrt((Ph ** 2).sum(axis=0) / (Ph.shape[0] - 1))
+        sd[sd == 0.0] = 1.0
+        Ph = Ph / sd
+        Z = np.concatenate([np.ones((keep.size, 1)), Ph], axis=1)
+        U, _, _ = np.linalg.svd(Z, full_matrices=False)
+        causal = np.sort(rng.choice(m, size=n_causal, replace=False))
+        crow = packed_dev[torch.as_tensor(causal, device=dev)].cpu().numpy().view(np.uint64)
+        g = rng.standard_normal(n_causal) @ synth.unpack_rows(crow, n)[:, keep].astype(np.float64)
+        y = g + 0.5 * Ph[:, -1] + rng.standard_normal(keep.size)
+        out.append((np.ascontiguousarray(U), y, keep))
+    return out
+
+
+def lognormal_shards(m: int, lo: int, hi: int, seed: int) -> np.ndarray:
+    """Start offsets of shards of lognormal length clipped to [lo, hi] covering m k-mers."""
+    rng = np.random.default_rng(seed)
+    starts, s = [], 0
+    mu = np.log(np.sqrt(lo * hi))
+    while s < m:
+        starts.append(s)
+        s += int(np.clip(rng.lognormal(mu, 0.8), lo, hi))
+    return np.asarray(starts, dtype=np.uint64)
