@@ -121,8 +121,9 @@ int kg_run_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t n_kmers,
                 uint32_t words_per_kmer, kg_result* res, kg_stats* stats);
 
 /* Same on device-resident rows.  Enqueues the kernels on `stream`
- * (a cudaStream_t; NULL = the context's own stream) and returns without
- * synchronising; kg_fetch() waits and returns the result. */
+ * (a cudaStream_t; NULL selects the context's own stream, not the legacy
+ * default stream) and returns without synchronising; kg_fetch() waits and
+ * returns the result. */
 int kg_launch_device(kg_ctx* ctx, const uint64_t* d_xbits, uint64_t n_kmers,
                      uint32_t words_per_kmer, void* stream);
 int kg_fetch(kg_ctx* ctx, kg_result* res, kg_stats* stats);

@@ -122,7 +122,7 @@ int enqueue_multi(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, uns
   if (m == 0) return KG_OK;
   kg::DevOutMP O = dev_out(ctx, offset);
   KG_CUDA(cudaMemsetAsync(M.dCounters + 3, 0, sizeof(unsigned long long), st), "memset");
-  kg::LaunchMp L{dx, m, (int)wpk, M.kpad, M.NP, M.G, M.xs, M.nb, M.dB, M.dPh, &O, ctx->num_sms};
+  kg::LaunchMp L{dx, m, (int)wpk, M.kpad, M.NP, M.G, M.xs, M.nb, 0, 0, M.dB, M.dPh, &O, ctx->num_sms};
   cudaError_t e = kg::launch_mp(L, st);
   if (e != cudaSuccess) return ctx->cuda_fail(e, "multi-phenotype kernel launch");
   kg::LaunchMpRefine R{dx, (int)wpk, M.dV, M.nsteps * 128, M.cm, M.vstride, M.dPh, &O, ctx->num_sms};

@@ -7,14 +7,14 @@
 //   warps 0-3   epilogue: per phenotype of the group, limb recombination and
 //               the FP64 statistic (src/kgwas.cpp:44-56, 182-218); tested
 //               counts per (shard, phenotype), hit and refinement records;
-//   warps 4-19  unpack, four groups: 128 samples of the resident tile ->
+//   warps 4-11  unpack, two groups: 128 samples of the resident tile ->
 //               int8 (0 / -128) -> one TMEM A stage (tcgen05.st);
-//   warp 20     x producer: the tile's packed rows, one 2-D TMA load per
+//   warp 12     x producer: the tile's packed rows, one 2-D TMA load per
 //               1024 samples (128-byte swizzle, no multicast);
-//   warp 21     B producer: the int8 limbs of each phenotype group, one
+//   warp 13     B producer: the int8 limbs of each phenotype group, one
 //               128-sample x N chunk per bulk copy from L2 into a ring;
-//   warp 22     MMA: tcgen05.mma kind::i8, A from TMEM, B from the ring,
-//               into one of two TMEM accumulators (N = phenotypes per group x
+//   warp 14     MMA: tcgen05.mma kind::i8, A from TMEM, B from the ring,
+//               into split-K TMEM accumulators (N = phenotypes per group x
 //               slot width <= 128 columns).
 // Group gi of a tile re-unpacks the tile (cheap: it is on chip) while the
 // previous group's accumulator is drained by the epilogue.
@@ -28,7 +28,7 @@ namespace kg {
 
 constexpr int MP_TM = 128;
 constexpr int MP_KS = 128;
-constexpr int MP_UG = 4;
+constexpr int MP_UG = 2;
 constexpr int MP_LU = 3, MP_LY = 5;
 constexpr int MP_WARP_UNPACK0 = 4, MP_WARP_XP = 4 + 4 * MP_UG, MP_WARP_BP = MP_WARP_XP + 1,
               MP_WARP_MMA = MP_WARP_BP + 1;
@@ -36,8 +36,11 @@ constexpr int MP_THREADS = 32 * (MP_WARP_MMA + 1);
 constexpr uint32_t MP_BOXB = MP_TM * 128;  // one TMA box: 128 rows x 128 bytes
 constexpr unsigned long long MP_KMER_MASK = (1ull << 48) - 1;
 
-__host__ __device__ constexpr int mp_a0(int N) { return ((2 * N + 31) / 32) * 32; }
-__host__ __device__ constexpr int mp_ast(int N) { return (512 - mp_a0(N)) / 32 > 16 ? 16 : (512 - mp_a0(N)) / 32; }
+// TMEM: NA accumulator buffers x S split-K accumulators x N columns, then A stages.
+__host__ __device__ constexpr int mp_a0(int N, int S, int NA) { return ((NA * S * N + 31) / 32) * 32; }
+__host__ __device__ constexpr int mp_ast(int N, int S, int NA) {
+  return (512 - mp_a0(N, S, NA)) / 32 > 16 ? 16 : (512 - mp_a0(N, S, NA)) / 32;
+}
 
 struct MpSmem {
   uint32_t x, b, bars, tmem, abort, total;
@@ -137,12 +140,12 @@ __device__ __forceinline__ void mp_eval(const EpiParams& P, bool valid, int c, d
 template <int NP>
 __global__ void __launch_bounds__(MP_THREADS, 1)
     mp_kernel(const __grid_constant__ CUtensorMap tmap, unsigned long long m, int nbox, int nchunk, int G,
-              int xs_slots, int nb, const int8_t* __restrict__ Bimg, const MPheno* __restrict__ ph,
+              int xs_slots, int nb, int S, int NA, const int8_t* __restrict__ Bimg, const MPheno* __restrict__ ph,
               const DevOutMP O) {
   constexpr int PPG = 128 / NP;
   constexpr int N = PPG * NP;
-  constexpr int A0 = mp_a0(N);
-  constexpr int AST = mp_ast(N);
+  const int A0 = mp_a0(N, S, NA);
+  const int AST = mp_ast(N, S, NA);
   constexpr uint32_t IDESC = idesc_i8(MP_TM, N);
   constexpr uint32_t BCH = 128u * N;  // bytes of one B chunk (128 samples x N)
   constexpr int KU_MAX = (NP - 1 - MP_LY) / MP_LU;
@@ -179,7 +182,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
       mbar_init(a_full + 8 * t, 4);
       mbar_init(a_empty + 8 * t, 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < NA; ++b) {
       mbar_init(acc_full + 8 * b, 1);
       mbar_init(acc_empty + 8 * b, 4);
     }
@@ -239,7 +242,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
       bool ok = true;
       for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         for (int gi = 0; gi < G && ok; ++gi, ++w) {
-          const uint32_t b = w & 1, v = w >> 1;
+          const uint32_t b = w % NA, v = w / NA;
           if (v > 0 && !mp_wait(acc_empty + 8 * b, (v - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA)) {
             ok = false;
             break;
@@ -253,10 +256,11 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
               break;
             }
             tc_fence_after();
+            const uint32_t d_t = tmem + (b * S + kc % S) * N;  // split-K accumulator of this stage
 #pragma unroll
             for (int ks = 0; ks < MP_KS / 32; ++ks) {
               const uint64_t bd = sdesc_noswz(sb + s * BCH + ks * 2 * (N * 16), N * 16, 128);
-              tc_mma_i8_ts(tmem + b * N, tmem + A0 + t * 32 + ks * 8, bd, IDESC, (kc | ks) != 0);
+              tc_mma_i8_ts(d_t, tmem + A0 + t * 32 + ks * 8, bd, IDESC, (kc >= S || ks != 0) ? 1u : 0u);
             }
             tc_commit(a_empty + 8 * t);
             tc_commit(b_empty + 8 * s);
@@ -316,6 +320,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
     const int q = warp & 3;
     const int r = q * 32 + lane;
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+    const int nsplit = nchunk < S ? nchunk : S;
     uint32_t w = 0;
     bool ok = true;
     for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
@@ -326,7 +331,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
       const unsigned match = __match_any_sync(0xffffffffu, shard);
       const bool leader = lane == __ffs(match) - 1;
       for (int gi = 0; gi < G; ++gi, ++w) {
-        const uint32_t b = w & 1, v = w >> 1;
+        const uint32_t b = w % NA, v = w / NA;
         if (!__all_sync(0xffffffffu, mp_wait(acc_full + 8 * b, v & 1, s_abort, O.counters, ERR_TIMEOUT_MMA))) {
           ok = false;
           break;
@@ -336,15 +341,22 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
           const int p = gi * PPG + pp;
           if (p >= O.n_pheno) break;
           // this phenotype's slot of the accumulator: NP int32 columns
+          // sum of the split-K partial accumulators of this slot
           uint32_t d[NP];
 #pragma unroll
           for (int c16 = 0; c16 < NP / 16; ++c16) {
             uint32_t rr[16];
-            tc_ld16(tmem + lane_base + b * N + pp * NP + c16 * 16, rr);
+            tc_ld16(tmem + lane_base + b * S * N + pp * NP + c16 * 16, rr);
+            tc_wait_ld();
 #pragma unroll
             for (int e = 0; e < 16; ++e) d[c16 * 16 + e] = rr[e];
+            for (int sp = 1; sp < nsplit; ++sp) {
+              tc_ld16(tmem + lane_base + (b * S + sp) * N + pp * NP + c16 * 16, rr);
+              tc_wait_ld();
+#pragma unroll
+              for (int e = 0; e < 16; ++e) d[c16 * 16 + e] += rr[e];
+            }
           }
-          tc_wait_ld();
           const MPheno& ME = ph[p];
           const int k = ME.P.k;
           const int drop0 = ME.drop0;
@@ -538,8 +550,13 @@ static cudaError_t launch_mp_t(const LaunchMp& L, const CUtensorMap& tm, cudaStr
   const unsigned long long tiles = (L.m + MP_TM - 1) / MP_TM;
   unsigned long long grid = (unsigned long long)L.num_sms;
   if (grid > tiles) grid = tiles;
-  mp_kernel<NP><<<(unsigned)grid, MP_THREADS, smem, st>>>(tm, L.m, nbox, L.kpad / MP_KS, L.G, L.xs, L.nb, L.Bimg,
-                                                          L.ph, *L.O);
+  int S = L.splits, NA = L.nacc;
+  if (S < 1 || NA < 1 || mp_ast(N, S, NA) < 4) {  // default: independent chains beside >= 8 A stages
+    S = N <= 64 ? 4 : 2;
+    NA = (N <= 32 || (N > 64 && N <= 80)) ? 2 : 1;
+  }
+  mp_kernel<NP><<<(unsigned)grid, MP_THREADS, smem, st>>>(tm, L.m, nbox, L.kpad / MP_KS, L.G, L.xs, L.nb, S, NA,
+                                                          L.Bimg, L.ph, *L.O);
   return cudaGetLastError();
 }
 

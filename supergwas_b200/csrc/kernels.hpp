@@ -60,6 +60,7 @@ struct LaunchMp {
   int NP;                     // columns per phenotype slot (multiple of 16, <= 128)
   int G;                      // phenotype groups (128 / NP phenotypes each)
   int xs, nb;                 // resident x tiles (1-2), B ring stages (2-8)
+  int splits, nacc;           // split-K accumulators, accumulator buffers (0: default)
   const int8_t* Bimg;         // G x (kpad/128) chunks of 128 x N bytes (device)
   const MPheno* ph;           // per-phenotype constants (device)
   const DevOutMP* O;

@@ -32,7 +32,7 @@ def main():
     wpk = X.shape[1]
     g = api.Kgwas(precision="fp64" if a.kernel == "fp64" else "split", corr_threshold=0.0, log10_thresh=6.0)
     g.set_structure(U, y, keep, a.n)
-    st = torch.cuda.current_stream()
+    st = torch.cuda.Stream()  # a real stream handle (NULL would select the context's own stream)
     g.launch_device(X.data_ptr(), a.kmers, wpk, st.cuda_stream)  # warm-up
     g.fetch()
     torch.cuda.synchronize()

@@ -35,8 +35,8 @@ def gen_packed(n: int, m: int, S: int, seed: int, device: str = "cuda", chunk: i
         p = p.clamp(1e-6, 1 - 1e-6)
         a = (p * c).unsqueeze(1).expand(cm, S)
         b = ((1 - p) * c).unsqueeze(1).expand(cm, S)
-        ga = torch._standard_gamma(a.contiguous())
-        gb = torch._standard_gamma(b.contiguous())
+        ga = torch._standard_gamma(a.contiguous(), generator=g)
+        gb = torch._standard_gamma(b.contiguous(), generator=g)
         ps = torch.nan_to_num(ga / (ga + gb), nan=0.5).to(torch.float32)
         probs = ps[:, pop]                                   # (cm, n)
         bits = torch.rand(cm, n, generator=g, device=device, dtype=torch.float32) < probs
