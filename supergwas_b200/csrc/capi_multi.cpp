@@ -424,30 +424,88 @@ int kg_run_multi_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t w
                       int n_shards, kg_multi_result* res) {
   if (!ctx) return KG_ERR_INVALID;
   KG_CUDA(cudaSetDevice(ctx->opts.device), "cudaSetDevice");
-  if (m == 0) {
-    Multi& M = ctx->mp;
-    int rc = check_multi(ctx, xbits, 0, wpk);
-    if (rc) return rc;
-    if ((rc = set_shards(ctx, shard_start, n_shards, 0))) return rc;
-    if ((rc = ensure_multi_out(ctx, M.n_shards, std::max<unsigned long long>(M.hit_cap, 1ull << 16)))) return rc;
-    if ((rc = reset_outputs(ctx, ctx->stream))) return rc;
-    KG_CUDA(cudaStreamSynchronize(ctx->stream), "sync");
-    std::memset(M.counters, 0, sizeof(M.counters));
-    return collect_multi(ctx, 0, res);
+  Multi& M = ctx->mp;
+  int rc = check_multi(ctx, xbits, m, wpk);
+  if (rc) return rc;
+  if ((rc = set_shards(ctx, shard_start, n_shards, m))) return rc;
+  if ((rc = ensure_multi_out(ctx, M.n_shards, std::max<unsigned long long>(M.hit_cap, 1ull << 16)))) return rc;
+  if (!ctx->dCand || ctx->cand_cap < (1ull << 20)) {
+    dfree(ctx->dCand);
+    KG_CUDA(cudaMalloc((void**)&ctx->dCand, (1ull << 20) * sizeof(unsigned long long)), "cudaMalloc(candidates)");
+    ctx->cand_cap = 1ull << 20;
   }
-  // Stage the rows on the device in one buffer, then one launch over all of them.
-  uint64_t* dx = nullptr;
-  const size_t bytes = (size_t)m * wpk * 8;
-  KG_CUDA(cudaMalloc((void**)&dx, bytes), "cudaMalloc(rows)");
-  cudaError_t e = cudaMemcpyAsync(dx, xbits, bytes, cudaMemcpyHostToDevice, ctx->stream);
-  int rc = e == cudaSuccess ? kg_launch_multi_device(ctx, dx, m, wpk, shard_start, n_shards, ctx->stream)
-                            : ctx->cuda_fail(e, "H2D");
-  if (!rc) rc = kg_fetch_multi(ctx, res);
-  cudaStreamSynchronize(ctx->stream);
-  drop_graph(ctx->mp);
-  ctx->mp.g_x = nullptr;
-  cudaFree(dx);
-  return rc;
+  cudaStream_t st = ctx->stream;
+  KG_CUDA(cudaMemcpyAsync(M.dShard, M.shard_host.data(), M.shard_host.size() * sizeof(unsigned long long),
+                          cudaMemcpyHostToDevice, st),
+          "copy shards");
+  ctx->launches = 0;
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    if ((rc = reset_outputs(ctx, st))) return rc;
+    // Chunks of the rows stream through two device buffers: the copy of
+    // chunk i+1 (copy stream) overlaps the kernels of chunk i (compute stream).
+    const size_t row = (size_t)wpk * 8;
+    size_t want = (size_t)4096 << 20;
+    if (const char* v = std::getenv("KG_CHUNK_MB")) want = (size_t)std::max(1, std::atoi(v)) << 20;
+    uint64_t per = std::max<uint64_t>(1, want / row);
+    if (per > m) per = m;
+    const size_t bytes = (size_t)per * row;
+    cudaPointerAttributes attr{};
+    const bool pinned = m == 0 || (cudaPointerGetAttributes(&attr, xbits) == cudaSuccess &&
+                                   (attr.type == cudaMemoryTypeHost || attr.type == cudaMemoryTypeManaged));
+    cudaGetLastError();
+    if (ctx->chunk_bytes < bytes) {
+      for (int b = 0; b < NBUF; ++b) {
+        dfree(ctx->dChunk[b]);
+        if (ctx->hStage[b]) cudaFreeHost(ctx->hStage[b]);
+        ctx->hStage[b] = nullptr;
+      }
+      ctx->chunk_bytes = 0;
+      for (int b = 0; b < NBUF; ++b) KG_CUDA(cudaMalloc((void**)&ctx->dChunk[b], bytes), "cudaMalloc(chunk)");
+      ctx->chunk_bytes = bytes;
+    }
+    if (!pinned)
+      for (int b = 0; b < NBUF; ++b)
+        if (!ctx->hStage[b])
+          KG_CUDA(cudaHostAlloc(&ctx->hStage[b], ctx->chunk_bytes, cudaHostAllocDefault), "cudaHostAlloc");
+    const uint64_t nch = m ? (m + per - 1) / per : 0;
+    for (uint64_t i = 0; i < nch; ++i) {
+      const int b = (int)(i % NBUF);
+      const uint64_t s0 = i * per, cnt = std::min<uint64_t>(per, m - s0);
+      const size_t nb = (size_t)cnt * row;
+      const char* src = (const char*)xbits + (size_t)s0 * row;
+      if (i >= (uint64_t)NBUF) {
+        KG_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_k[b], 0), "wait");
+        if (!pinned) KG_CUDA(cudaEventSynchronize(ctx->ev_h2d[b]), "sync");
+      }
+      if (!pinned) {
+        std::memcpy(ctx->hStage[b], src, nb);
+        src = (const char*)ctx->hStage[b];
+      }
+      KG_CUDA(cudaMemcpyAsync(ctx->dChunk[b], src, nb, cudaMemcpyHostToDevice, ctx->copy_stream), "H2D");
+      KG_CUDA(cudaEventRecord(ctx->ev_h2d[b], ctx->copy_stream), "record");
+      KG_CUDA(cudaStreamWaitEvent(st, ctx->ev_h2d[b], 0), "wait");
+      if (i == 0 && (rc = autotune(ctx, ctx->dChunk[b], cnt, wpk, st))) return rc;
+      if (i == 0 && (rc = reset_outputs(ctx, st))) return rc;  // the autotuner's trial launches wrote outputs
+      if ((rc = enqueue_multi(ctx, ctx->dChunk[b], cnt, wpk, s0, st))) return rc;
+      KG_CUDA(cudaEventRecord(ctx->ev_k[b], st), "record");
+    }
+    KG_CUDA(cudaMemcpyAsync(M.counters, M.dCounters, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
+            "copy counters");
+    KG_CUDA(cudaStreamSynchronize(st), "kernel");
+    if (!(M.counters[2] & (kg::ERR_HIT_OVERFLOW | kg::ERR_CAND_OVERFLOW))) break;
+    if ((M.counters[2] & kg::ERR_HIT_OVERFLOW) && (rc = ensure_multi_out(ctx, M.n_shards, M.counters[1])))
+      return rc;
+    if (M.counters[2] & kg::ERR_CAND_OVERFLOW) {
+      const unsigned long long cap = 4 * ctx->cand_cap;
+      dfree(ctx->dCand);
+      ctx->cand_cap = 0;
+      KG_CUDA(cudaMalloc((void**)&ctx->dCand, cap * sizeof(unsigned long long)), "cudaMalloc(candidates)");
+      ctx->cand_cap = cap;
+    }
+  }
+  drop_graph(M);
+  M.g_x = nullptr;
+  return collect_multi(ctx, m, res);
 }
 
 }  // extern "C"

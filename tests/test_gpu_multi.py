@@ -96,3 +96,18 @@ def test_multi_graph_replay(built):
     for t, h in outs[1:]:
         assert np.array_equal(t, outs[0][0])
         assert np.array_equal(h, outs[0][1])
+
+
+def test_multi_streamed_chunks_match_single_chunk(built, monkeypatch):
+    """Host rows streamed in many chunks through two device buffers give the
+    same counts and rows as one chunk (shard boundaries inside chunks)."""
+    n_all, m = 1000, 40000
+    packed, phenos = make_batch(n_all, m, 3, (8,), seed=19)
+    shards = np.array([0, 1000, 13333, 27001], dtype=np.uint64)
+    with api.Kgwas(corr_threshold=0.0, log10_thresh=1.0) as g:
+        g.set_phenotypes(phenos, n_all)
+        t1, h1 = g.run_multi_host(packed, shards)
+        monkeypatch.setenv("KG_CHUNK_MB", "1")      # 128-byte rows: 8192 k-mers per chunk
+        t2, h2 = g.run_multi_host(packed, shards)
+    assert np.array_equal(t1, t2)
+    assert np.array_equal(h1, h2)
