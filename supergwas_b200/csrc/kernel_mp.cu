@@ -551,9 +551,9 @@ static cudaError_t launch_mp_t(const LaunchMp& L, const CUtensorMap& tm, cudaStr
   unsigned long long grid = (unsigned long long)L.num_sms;
   if (grid > tiles) grid = tiles;
   int S = L.splits, NA = L.nacc;
-  if (S < 1 || NA < 1 || mp_ast(N, S, NA) < 4) {  // default: independent chains beside >= 8 A stages
-    S = N <= 64 ? 4 : 2;
-    NA = (N <= 32 || (N > 64 && N <= 80)) ? 2 : 1;
+  if (S < 1 || NA < 1 || mp_ast(N, S, NA) < 4) {  // default: one chain, two accumulator buffers
+    S = 1;
+    NA = 2;
   }
   mp_kernel<NP><<<(unsigned)grid, MP_THREADS, smem, st>>>(tm, L.m, nbox, L.kpad / MP_KS, L.G, L.xs, L.nb, S, NA,
                                                           L.Bimg, L.ph, *L.O);

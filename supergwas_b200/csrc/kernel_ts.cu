@@ -356,10 +356,11 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // Split-K accumulators and accumulator buffers for width N (KG_TS_SPLIT=
-// "S,NB" overrides): as many independent chains as fit beside 8 A stages.
+// "S,NB" overrides).
 static void ts_shape(int N, int& S, int& NB) {
-  S = N <= 32 ? 4 : N <= 64 ? 4 : 2;
-  NB = N <= 32 ? 2 : 1;
+  // measured on the 200M-k-mer workload: one chain, two buffers is fastest
+  S = 1;
+  NB = 2;
   if (const char* v = std::getenv("KG_TS_SPLIT")) {
     int s = 0, b = 0;
     if (std::sscanf(v, "%d,%d", &s, &b) == 2 && s >= 1 && s <= 8 && b >= 1 && b <= 2 &&

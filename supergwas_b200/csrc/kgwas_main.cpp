@@ -10,7 +10,13 @@
 // reference ignores:
 //   KGWAS_PRECISION  split (default: tcgen05 int8 limbs) | fp64 (CUDA cores)
 //   KGWAS_DEVICE     CUDA device ordinal (default 0)
+//   KGWAS_KBITS      1: keep the packed rows of the batch in a sidecar file
+//                    <batch>/kgwas_<N>_<n>_<hash>.kbits (hash of the overlap
+//                    sample positions) and reuse it instead of re-reading the
+//                    n ASCII/gz column files
+#include <fcntl.h>
 #include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <cmath>
@@ -178,6 +184,63 @@ static void format_hits(const kg_result& r, const vector<string>& kmers, const u
   two = o2.str();
 }
 
+// ---------------------------------------------------------- .kbits cache
+// 64-byte header: "KGWASKB1", N, n, words_per_kmer, FNV-1a of the overlap
+// positions; then N * words_per_kmer little-endian uint64 words.
+struct KbitsHeader {
+  char magic[8];
+  uint64_t N;
+  uint32_t n, wpk;
+  uint64_t idx_hash;
+  char pad[32];
+};
+static_assert(sizeof(KbitsHeader) == 64, "kbits header");
+
+static uint64_t fnv1a(const vector<int>& v) {
+  uint64_t h = 1469598103934665603ull;
+  for (int x : v)
+    for (int b = 0; b < 4; ++b) {
+      h ^= (uint64_t)((x >> (8 * b)) & 0xff);
+      h *= 1099511628211ull;
+    }
+  return h;
+}
+
+static string kbits_path(const string& batch, size_t N, int n, uint64_t h) {
+  char buf[96];
+  std::snprintf(buf, sizeof(buf), "/kgwas_%zu_%d_%016llx.kbits", N, n, (unsigned long long)h);
+  return batch + buf;
+}
+
+static bool kbits_read(const string& path, size_t N, int n, uint32_t W, uint64_t h, uint64_t* out) {
+  std::ifstream in(path, std::ios::binary);
+  if (!in) return false;
+  KbitsHeader hd{};
+  in.read((char*)&hd, sizeof(hd));
+  if (!in || std::memcmp(hd.magic, "KGWASKB1", 8) != 0 || hd.N != N || hd.n != (uint32_t)n || hd.wpk != W ||
+      hd.idx_hash != h)
+    return false;
+  in.read((char*)out, (std::streamsize)(N * W * 8));
+  return (bool)in;
+}
+
+static void kbits_write(const string& path, size_t N, int n, uint32_t W, uint64_t h, const uint64_t* x) {
+  const string tmp = path + ".tmp." + std::to_string(::getpid());
+  std::ofstream out(tmp, std::ios::binary);
+  if (!out) return;
+  KbitsHeader hd{};
+  std::memcpy(hd.magic, "KGWASKB1", 8);
+  hd.N = N;
+  hd.n = (uint32_t)n;
+  hd.wpk = W;
+  hd.idx_hash = h;
+  out.write((const char*)&hd, sizeof(hd));
+  out.write((const char*)x, (std::streamsize)(N * W * 8));
+  out.close();
+  if (out) std::rename(tmp.c_str(), path.c_str());
+  else std::remove(tmp.c_str());
+}
+
 static void run_cols(const Config& cfg) {  // src/kgwas.cpp:168-307
   kgio::Timer tall;
   kgio::Overlap ov = kgio::build_overlap(cfg.samples_file, cfg.pheno_file);
@@ -190,7 +253,16 @@ static void run_cols(const Config& cfg) {  // src/kgwas.cpp:168-307
   const uint32_t W = kgio::words_per_kmer(n);
   HostWords X;
   X.alloc((size_t)N * W);
-  kgio::load_matrix_packed(bits_dir, ov.idxs, N, cfg.LOAD_THREADS, X.p);
+  const char* kb = std::getenv("KGWAS_KBITS");
+  const bool use_kbits = kb && std::string(kb) == "1";
+  const uint64_t h = fnv1a(ov.idxs);
+  const string kpath = kbits_path(cfg.input_path, N, n, h);
+  if (use_kbits && kbits_read(kpath, N, n, W, h, X.p)) {
+    std::cerr << "[INFO] packed rows from " << kpath << "\n";
+  } else {
+    kgio::load_matrix_packed(bits_dir, ov.idxs, N, cfg.LOAD_THREADS, X.p);
+    if (use_kbits) kbits_write(kpath, N, n, W, h, X.p);
+  }
 
   Gpu g;
   g.open(cfg);
