@@ -17,6 +17,17 @@ __device__ __forceinline__ unsigned long long gtimer_ns() {
   return t;
 }
 
+// Exact int64 -> double for |v| < 2^51 without the conversion unit: the
+// double 1.5 * 2^52 has unit spacing and a zero low 51-bit mantissa field, so
+// adding v to its bit pattern yields the double 1.5 * 2^52 + v exactly
+// ("magic number" conversion, Hacker's Delight ch. 17 style).  The caller
+// subtracts the bias, usually folded into an FMA.
+constexpr double MAGIC_BIAS = 6755399441055744.0;  // 1.5 * 2^52
+__device__ __forceinline__ double magic_raw(long long v) {
+  return __longlong_as_double(0x4338000000000000LL + v);
+}
+__device__ __forceinline__ double i2d_exact(long long v) { return magic_raw(v) - MAGIC_BIAS; }
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
@@ -258,8 +269,9 @@ __device__ __forceinline__ void finish_kmer_fast(const EpiParams& P, const DevOu
   double xxM = 0, xyM = 0, effect = 0, T = 0, p = 1;
   bool cand = false, hit = false;
   if (tested) {
-    xxM = (double)c - ss;
-    xyM = P.b * (double)c + ey;
+    const double cd = i2d_exact(c);
+    xxM = cd - ss;
+    xyM = P.b * cd + ey;
     const double eps = 1e-12;
     if (xxM > eps && P.yyM > eps) {
       const double q = xyM * xyM, den = xxM * P.yyM;

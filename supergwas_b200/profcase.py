@@ -47,8 +47,7 @@ def main():
     times.sort()
     med = times[len(times) // 2]
     print(f"kernel={g.last_kernel()} kmers={a.kmers} tested={r.n_tested} hits={r.hits.shape[0]} "
-          f"device_ms_per_launch={med:.3f} kmers_per_s={a.kmers / med * 1e3:.4g} "
-          f"split={os.environ.get('KG_TS_SPLIT', 'default')}")
+          f"device_ms_per_launch={med:.3f} kmers_per_s={a.kmers / med * 1e3:.4g}")
     g.close()
 
 
