@@ -210,43 +210,61 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     }
   } else if (warp == TS_WARP_MMA) {
     // ----------------------------------------------------------------- MMA
-    if (lane == 0) {
-      bool ok = ts_wait(b_full, 0, s_abort, O.counters, ERR_TIMEOUT_FULL);
-      const uint64_t bdesc0 = sdesc_noswz(sb, N * 16, 128);
-      Ring<NSLOT> ar;
-      uint32_t i = 0;
-      for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++i) {
-        const uint32_t b = i & 1u;
-        if (i >= 2 && !ts_wait(acc_empty + 8 * b, ((i >> 1) - 1) & 1u, s_abort, O.counters, ERR_TIMEOUT_MMA)) {
+    // The whole warp runs the loop (warp-uniform control flow and operands);
+    // one elected lane issues the MMAs and the commits that track them.
+    const bool leader = elect_one();
+    bool ok = __all_sync(0xffffffffu, ts_wait(b_full, 0, s_abort, O.counters, ERR_TIMEOUT_FULL));
+    const uint64_t bdesc0 = sdesc_noswz(sb, N * 16, 128);
+    Ring<NSLOT> ar;
+    uint32_t i = 0;
+    for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++i) {
+      const uint32_t b = i & 1u;
+      if (i >= 2 && !__all_sync(0xffffffffu, ts_wait(acc_empty + 8 * b, ((i >> 1) - 1) & 1u, s_abort, O.counters,
+                                                     ERR_TIMEOUT_MMA))) {
+        ok = false;
+        break;
+      }
+      const uint32_t d_t = tmem + b * N;
+      uint64_t bd = bdesc0;
+      for (int sp = 0; sp < nsp; ++sp, ar.next()) {
+        if (!__all_sync(0xffffffffu, ts_wait(a_full + 8 * ar.slot, ar.phase, s_abort, O.counters, ERR_TIMEOUT_MMA))) {
           ok = false;
           break;
         }
-        const uint32_t d_t = tmem + b * N;
-        uint64_t bd = bdesc0;
-        for (int sp = 0; sp < nsp; ++sp, ar.next()) {
-          if (!ts_wait(a_full + 8 * ar.slot, ar.phase, s_abort, O.counters, ERR_TIMEOUT_MMA)) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-          const int nsub_here = nsub - sp * TS_SUPER < TS_SUPER ? nsub - sp * TS_SUPER : TS_SUPER;
-          const uint32_t a_t = tmem + A0 + ar.slot * 128;
-          for (int sub = 0; sub < nsub_here; ++sub) {
+        tc_fence_after();
+        const int nsub_here = nsub - sp * TS_SUPER < TS_SUPER ? nsub - sp * TS_SUPER : TS_SUPER;
+        const uint32_t a_t = tmem + A0 + ar.slot * 128;
+        if (leader) {
+          if (nsub_here == TS_SUPER) {
+            // full super-stage: 16 MMAs with compile-time operand offsets
 #pragma unroll
-            for (int ks = 0; ks < TS_KS / 32; ++ks) {
-              tc_mma_i8_ts(d_t, a_t + sub * 32 + ks * 8, bd, IDESC, (sp | sub | ks) ? 1u : 0u);
-              bd += BSTEP;
+            for (int k = 0; k < TS_SUPER * (TS_KS / 32); ++k)
+              tc_mma_i8_ts(d_t, a_t + k * 8, bd + (uint64_t)(k * BSTEP), IDESC, (sp | k) ? 1u : 0u);
+          } else {
+            uint64_t bk = bd;
+            for (int sub = 0; sub < nsub_here; ++sub) {
+#pragma unroll
+              for (int ks = 0; ks < TS_KS / 32; ++ks) {
+                tc_mma_i8_ts(d_t, a_t + sub * 32 + ks * 8, bk, IDESC, (sp | sub | ks) ? 1u : 0u);
+                bk += BSTEP;
+              }
             }
           }
           tc_commit(a_empty + 8 * ar.slot);
         }
-        if (!ok) break;
-        tc_commit(acc_full + 8 * b);
+        __syncwarp();
+        bd += (uint64_t)(TS_SUPER * (TS_KS / 32) * BSTEP);
       }
-      // drain: wait (bounded) until every issued MMA has completed
+      if (!ok) break;
+      if (leader) tc_commit(acc_full + 8 * b);
+      __syncwarp();
+    }
+    // drain: wait (bounded) until every issued MMA has completed
+    if (leader) {
       tc_commit(drain);
       mbar_wait(drain, 0, O.counters, ERR_TIMEOUT_MMA);
     }
+    __syncwarp();
   } else if (warp >= TS_WARP_UNPACK0) {
     // -------------------------------------------------------------- unpack
     const int q = warp & 3;                    // TMEM lane quarter
