@@ -184,6 +184,7 @@ int kg_set_structure_ex(kg_ctx* ctx, const double* U, int n, int k, const double
       LM.nl[j] = ctx->limbs.nl[j];
       LM.scale[j] = ctx->limbs.scale[j];
     }
+    kg::set_limb_consts(LM);
     dfree(ctx->dB);
     KG_CUDA(cudaMalloc((void**)&ctx->dB, img.size()), "cudaMalloc(B)");
     KG_CUDA(cudaMemcpy(ctx->dB, img.data(), img.size(), cudaMemcpyHostToDevice), "copy B");

@@ -301,6 +301,7 @@ int kg_set_phenotypes(kg_ctx* ctx, const kg_pheno* ph, int np, int n_row) {
       LM.nl[j] = limbs[p].nl[j];
       LM.scale[j] = limbs[p].scale[j];
     }
+    kg::set_limb_consts(LM);
     mph[p].drop0 = (k > 0 && prep[p].drop0) ? 1 : 0;
   }
   // FP64 refinement operands: per phenotype, rows = packed-row sample positions,

@@ -170,12 +170,11 @@ __device__ __forceinline__ double mlog10_sf(double T) {
 // Warp-aggregated outputs of one k-mer: tested count, hit record, FP64
 // refinement candidate, and (when requested) the per-k-mer arrays.  All 32
 // lanes of the warp must call it.
-__device__ __forceinline__ void emit_kmer(const DevOut& O, unsigned long long local, bool valid, bool tested,
-                                          bool hit, bool cand, double T, double p, double effect, double xxM,
-                                          double xyM, double cor) {
+// Warp-aggregated hit records and refinement candidates of one k-mer per
+// lane.  All 32 lanes of the warp must call it.
+__device__ __forceinline__ void emit_rare(const DevOut& O, unsigned long long local, bool hit, bool cand, double T,
+                                          double p, double effect) {
   const unsigned lane = threadIdx.x & 31u;
-  const unsigned tmask = __ballot_sync(0xffffffffu, tested);
-  if (lane == 0 && tmask) atomicAdd(O.counters + 0, (unsigned long long)__popc(tmask));
   const unsigned hmask = __ballot_sync(0xffffffffu, hit);
   if (hmask) {
     unsigned long long base = 0;
@@ -208,6 +207,15 @@ __device__ __forceinline__ void emit_kmer(const DevOut& O, unsigned long long lo
       else atomicOr(O.counters + 2, (unsigned long long)ERR_CAND_OVERFLOW);
     }
   }
+}
+
+__device__ __forceinline__ void emit_kmer(const DevOut& O, unsigned long long local, bool valid, bool tested,
+                                          bool hit, bool cand, double T, double p, double effect, double xxM,
+                                          double xyM, double cor) {
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned tmask = __ballot_sync(0xffffffffu, tested);
+  if (lane == 0 && tmask) atomicAdd(O.counters + 0, (unsigned long long)__popc(tmask));
+  emit_rare(O, local, hit, cand, T, p, effect);
   if (valid && O.tested) {
     const unsigned long long g = O.kmer_offset + local;
     O.tested[g] = tested ? 1 : 0;
@@ -299,6 +307,49 @@ __device__ __forceinline__ void finish_kmer_fast(const EpiParams& P, const DevOu
     }
   }
   emit_kmer(O, local, valid, tested, hit, cand, T, p, effect, xxM, xyM, 0.0);
+}
+
+// Fast screen of one k-mer for kernels that count tested k-mers in a
+// register (tested_local, flushed once per warp by the caller): in the common
+// case (no hit, no refinement candidate in the warp) it costs one ballot.
+// Same decisions and values as finish_kmer_fast.
+__device__ __forceinline__ void finish_kmer_lean(const EpiParams& P, const DevOut& O, unsigned long long local,
+                                                 bool valid, int c, double cd, double ss, double gs, double ey,
+                                                 uint32_t& tested_local) {
+  const int n = P.n;
+  bool tested = valid && c > 0 && c < n && !(P.ynorm < 1e-12);
+  if (P.corr_thr > 0.0) {
+    const double xcn2 = cd * (double)(n - c) / (double)n;
+    const double xyc = ey + gs + P.kappa * cd;
+    tested = tested && xyc * xyc >= P.thr2_ynorm2 * xcn2;
+  }
+  tested_local += tested ? 1u : 0u;
+  const double eps = 1e-12;
+  const double xxM = cd - ss;
+  const double xyM = P.b * cd + ey;
+  const double q = xyM * xyM, den = xxM * P.yyM;
+  const bool ok = tested && xxM > eps && P.yyM > eps;
+  const bool cand = ok && P.refine && q >= P.r2_ref * den;
+  const bool maybe = ok && !cand && q >= P.r2_cand * den;
+  if (__ballot_sync(0xffffffffu, cand || maybe) == 0u) return;
+  double T = 0, p = 1, effect = 0;
+  bool hit = false;
+  if (maybe) {
+    double r2 = q / den;
+    if (r2 < 0) r2 = 0;
+    if (r2 >= 1) r2 = 1 - 1e-15;
+    T = (double)n * log(1.0 / (1.0 - r2));
+    p = erfc(sqrt(0.5 * T));
+    effect = xyM / den;
+    hit = p <= P.p_thresh;
+  }
+  emit_rare(O, local, hit, cand, T, p, effect);
+}
+
+// Adds the per-thread tested counts of a warp to counters[0].
+__device__ __forceinline__ void flush_tested(const DevOut& O, uint32_t tested_local) {
+  const unsigned tot = __reduce_add_sync(0xffffffffu, tested_local);
+  if ((threadIdx.x & 31u) == 0 && tot) atomicAdd(O.counters + 0, (unsigned long long)tot);
 }
 
 }  // namespace kg

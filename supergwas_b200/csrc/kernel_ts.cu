@@ -1,19 +1,21 @@
 // kernel_ts.cu -- split-precision association kernel with the unpacked x
 // operand held in tensor memory.
 //
-// One persistent CTA per SM, warp-specialised (448 threads):
+// One persistent CTA per SM, warp-specialised (576 threads; 448 for N > 80):
 //   warps 0-7   epilogue, two groups of four (one warp per TMEM lane quarter),
 //               group e owning accumulator buffer e, i.e. every other tile:
 //               tcgen05.ld of the int32 accumulators (one TMEM lane = one
 //               k-mer), exact limb recombination, FP64 statistics,
 //               warp-aggregated hit compaction;
-//   warps 8-11  unpack: read 128 samples of a packed row from the TMA-filled
-//               shared tile and write them as int8 (0 / -128) straight into a
-//               TMEM A slot with tcgen05.st -- the unpacked operand never
-//               touches shared memory;
-//   warp 12     producer: one 2-D TMA load (128 rows x 128 bytes, 128-byte
+//   warps 8-15  unpack, two groups of four taking super-stages in turn (one
+//               group for N > 80, so that the epilogue keeps its registers): read
+//               128 samples of a packed row from the TMA-filled shared tile
+//               and write them as int8 (0 / -128) straight into a TMEM A slot
+//               with tcgen05.st -- the unpacked operand never touches shared
+//               memory;
+//   warp 16     producer (12 for N > 80): one 2-D TMA load (128 rows x 128 bytes, 128-byte
 //               swizzle, no multicast) per 1024 samples of a 128-k-mer tile;
-//   warp 13     MMA: tcgen05.mma kind::i8, A from TMEM, B (the int8 limbs of
+//   warp 17     MMA (13 for N > 80): tcgen05.mma kind::i8, A from TMEM, B (the int8 limbs of
 //               the centred structure and phenotype columns, resident in
 //               shared memory for the whole launch) from a smem descriptor.
 // Tile = 128 k-mers (M), N = 16..128 limb columns.
@@ -45,10 +47,13 @@ constexpr int TS_KS = 128;         // samples per sub-stage (32 TMEM columns, 4 
 constexpr int TS_SUPER = 4;        // sub-stages per super-stage (one barrier, one commit)
 constexpr int TS_BOX = 1024;       // samples per TMA box (128 bytes)
 constexpr int TS_XST = 4;          // packed boxes in flight
-constexpr int TS_THREADS = 32 * 14;
+// Unpack groups (taking super-stages in turn): two while the epilogue fits
+// the register budget of 18 warps, one for wide N.
+__host__ __device__ constexpr int ts_ug(int N) { return N <= 80 ? 2 : 1; }
+__host__ __device__ constexpr int ts_threads(int N) { return 32 * (8 + 4 * ts_ug(N) + 2); }
 constexpr int TS_LU = 3, TS_LY = 5;
 constexpr uint32_t TS_XBYTES = TS_TM * 128;  // one box: 128 rows x 128 bytes
-constexpr int TS_WARP_UNPACK0 = 8, TS_WARP_PROD = 12, TS_WARP_MMA = 13;
+constexpr int TS_WARP_UNPACK0 = 8;  // then the unpack groups, the producer, the MMA warp
 constexpr int TS_MAXSLOT = 3;
 
 // Super-slots of 128 TMEM columns left after the two N-column accumulators.
@@ -123,10 +128,12 @@ struct Ring {
 };
 
 template <int N, bool DROP0>
-__global__ void __launch_bounds__(TS_THREADS, 1)
+__global__ void __launch_bounds__(ts_threads(N), 1)
     ts_kernel(const __grid_constant__ CUtensorMap tmap, unsigned long long m, int nbox, int nsub,
               const int8_t* __restrict__ Bimg, int b_bytes, const __grid_constant__ EpiParams P,
               const __grid_constant__ LimbMap LM, const DevOut O) {
+  constexpr int UG = ts_ug(N);
+  constexpr int TS_WARP_PROD = TS_WARP_UNPACK0 + 4 * UG, TS_WARP_MMA = TS_WARP_PROD + 1;
   constexpr int NSLOT = ts_nslot(N);
   constexpr int A0 = 512 - NSLOT * 128;  // first A column (>= 2N)
   static_assert(NSLOT >= 2 && A0 >= 2 * N, "TMEM budget");
@@ -156,10 +163,10 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
   if (tid == 32) {
     for (int s = 0; s < TS_XST; ++s) {
       mbar_init(x_full + 8 * s, 1);
-      mbar_init(x_empty + 8 * s, 4);  // the four unpack warps
+      mbar_init(x_empty + 8 * s, 4 * UG);  // every unpack warp
     }
     for (int t = 0; t < NSLOT; ++t) {
-      mbar_init(a_full + 8 * t, 4);   // the four unpack warps
+      mbar_init(a_full + 8 * t, 4);   // the four warps of one unpack group
       mbar_init(a_empty + 8 * t, 1);  // tcgen05.commit
     }
     for (int b = 0; b < 2; ++b) {
@@ -267,55 +274,88 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     __syncwarp();
   } else if (warp >= TS_WARP_UNPACK0) {
     // -------------------------------------------------------------- unpack
-    const int q = warp & 3;                    // TMEM lane quarter
-    const int r = q * 32 + lane;               // row of the tile = TMEM lane
+    const int grp = (warp - TS_WARP_UNPACK0) >> 2;  // takes every other super-stage
+    const int q = warp & 3;                         // TMEM lane quarter
+    const int r = q * 32 + lane;                    // row of the tile = TMEM lane
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
     Ring<TS_XST> xr;
     Ring<NSLOT> ar;
+    uint32_t turn = 0;  // super-stage counter parity
     bool ok = true;
     for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
       int kc = 0;  // sub-stage of the tile
       for (int bx = 0; bx < nbox && ok; ++bx, xr.next()) {
+        // every unpack warp waits for every box, also one holding none of its
+        // super-stages, so that its release below belongs to this fill
         if (!__all_sync(0xffffffffu, ts_wait(x_full + 8 * xr.slot, xr.phase, s_abort, O.counters,
                                             ERR_TIMEOUT_FULL))) {
           ok = false;
           break;
         }
-        const uint32_t xrow = sx + xr.slot * TS_XBYTES + r * 128;
         const int kc1 = (bx + 1) * (TS_BOX / TS_KS) < nsub ? (bx + 1) * (TS_BOX / TS_KS) : nsub;
         // super-stages never straddle a box: a box holds two of them
         while (kc < kc1) {
+          const int ke = kc + TS_SUPER < kc1 ? kc + TS_SUPER : kc1;
+          if (UG == 2 && turn != (uint32_t)grp) {  // the other group's super-stage
+            kc = ke;
+            ar.next();
+            turn ^= 1u;
+            continue;
+          }
           if (ar.used && !__all_sync(0xffffffffu, ts_wait(a_empty + 8 * ar.slot, ar.phase ^ 1u, s_abort,
                                                           O.counters, ERR_TIMEOUT_MMA))) {
             ok = false;
             break;
           }
-          const int ke = kc + TS_SUPER < kc1 ? kc + TS_SUPER : kc1;
+          const uint32_t xrow = sx + xr.slot * TS_XBYTES + r * 128;
           const uint32_t a_t = tmem + lane_base + A0 + ar.slot * 128;
-          for (int sub = 0; kc < ke; ++kc, ++sub) {
-            // 16 bytes (128 samples) of row r; 128-byte swizzle: chunk c of row r sits at c ^ (r % 8)
-            const int c = kc - bx * (TS_BOX / TS_KS);
-            uint4 v;
-            asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];"
-                         : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-                         : "r"(xrow + ((c ^ (r & 7)) << 4)));
-            const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
-            uint32_t o[32];
-            // byte t of column 8qq+j = bit 8t+j of word qq, moved to the byte's
-            // sign bit (0 or -128); the shift is a multiply so that it issues on
-            // the FMA pipe and the mask on the ALU pipe
+          const int c0 = kc - bx * (TS_BOX / TS_KS);
+          // 16 bytes (128 samples) of row r per sub-stage; 128-byte swizzle:
+          // chunk c of row r sits at c ^ (r % 8).  Byte t of column 8qq+j =
+          // bit 8t+j of word qq, moved to the byte's sign bit (0 or -128); the
+          // shift is a multiply so that it issues on the FMA pipe and the mask
+          // on the ALU pipe.
+          if (ke - kc == TS_SUPER) {
+            uint32_t w[TS_SUPER][4];
 #pragma unroll
-            for (int qq = 0; qq < 4; ++qq)
+            for (int sub = 0; sub < TS_SUPER; ++sub)
+              asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];"
+                           : "=r"(w[sub][0]), "=r"(w[sub][1]), "=r"(w[sub][2]), "=r"(w[sub][3])
+                           : "r"(xrow + (((c0 + sub) ^ (r & 7)) << 4)));
 #pragma unroll
-              for (int j = 0; j < 8; ++j) o[qq * 8 + j] = (w4[qq] * (1u << (7 - j))) & 0x80808080u;
-            tc_st32(a_t + sub * 32, o);
+            for (int sub = 0; sub < TS_SUPER; ++sub) {
+              uint32_t o[32];
+#pragma unroll
+              for (int qq = 0; qq < 4; ++qq)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) o[qq * 8 + j] = (w[sub][qq] * (1u << (7 - j))) & 0x80808080u;
+              tc_st32(a_t + sub * 32, o);
+            }
+          } else {
+            for (int sub = 0; sub < ke - kc; ++sub) {
+              uint4 v;
+              asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];"
+                           : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                           : "r"(xrow + (((c0 + sub) ^ (r & 7)) << 4)));
+              const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
+              uint32_t o[32];
+#pragma unroll
+              for (int qq = 0; qq < 4; ++qq)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) o[qq * 8 + j] = (w4[qq] * (1u << (7 - j))) & 0x80808080u;
+              tc_st32(a_t + sub * 32, o);
+            }
           }
+          kc = ke;
           tc_wait_st();
           tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive(a_full + 8 * ar.slot);
           ar.next();
+          if (UG == 2) turn ^= 1u;
         }
+        if (!ok) break;
+        // every unpack warp releases every box, whether or not it read from it
         __syncwarp();
         if (lane == 0) mbar_arrive(x_empty + 8 * xr.slot);
       }
@@ -326,7 +366,8 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     const int q = warp & 3;
     const int r = q * 32 + lane;
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
-    uint32_t jt = 0;  // tiles taken by this group
+    uint32_t jt = 0;            // tiles taken by this group
+    uint32_t tested_local = 0;  // k-mers this thread tested (lean path)
     for (unsigned long long tile = blockIdx.x + (unsigned long long)e * gridDim.x; tile < ntiles;
          tile += 2ull * gridDim.x, ++jt) {
       if (!__all_sync(0xffffffffu, ts_wait(acc_full + 8 * e, jt & 1u, s_abort, O.counters, ERR_TIMEOUT_MMA))) break;
@@ -349,7 +390,7 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
       // recombined exactly in int64 and turned into doubles with the
       // bias trick (integer add + one FMA, no conversion instructions):
       //   U column: V = sum_l 256^(L-1-l) d_l = -128 v, |V| < 2^41, and
-      //   e = round(V * (-scale/128)) = round(v * scale);
+      //   e = V * (-scale/128) = v * scale, exact (LimbMap esc/eoff);
       //   y':       |V| < 2^57, so v = -V >> 7 (exact) first.
       // The values equal those of the smem-A kernel bit for bit.
       const int c = (-(int)d[0]) >> 7;
@@ -364,24 +405,25 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
         const double s0 = P.a[0] * cd;
         ss = s0 * s0;
       }
+      // straight-line over every column slot that fits in N: slots past the
+      // phenotype's k columns have zero limbs and a = g = 0, so they add
+      // exact zeros
 #pragma unroll
       for (int jj = 0; jj < KU_MAX; ++jj) {
         const int j = jj + (DROP0 ? 1 : 0);
-        if (j < P.k) {
-          const int o = 1 + TS_LY + TS_LU * jj;
-          long long V = (int)d[o];
+        const int o = 1 + TS_LY + TS_LU * jj;
+        long long V = (int)d[o];
 #pragma unroll
-          for (int l = 1; l < TS_LU; ++l) V = V * 256 + (int)d[o + l];
-          const double sc = LM.scale[j] * -0.0078125;  // exact: scale is a power of two
-          const double e = fma(magic_raw(V), sc, -MAGIC_BIAS * sc);
-          const double sj = fma(P.a[j], cd, e);
-          ss = fma(sj, sj, ss);
-          gs = fma(P.g[j], e, gs);
-        }
+        for (int l = 1; l < TS_LU; ++l) V = V * 256 + (int)d[o + l];
+        const double e = fma(magic_raw(V), LM.esc[j], LM.eoff[j]);
+        const double sj = fma(P.a[j], cd, e);
+        ss = fma(sj, sj, ss);
+        gs = fma(P.g[j], e, gs);
       }
       if (O.tested) finish_kmer(P, O, local, valid, c, ss, gs, ey);
-      else finish_kmer_fast(P, O, local, valid, c, ss, gs, ey);
+      else finish_kmer_lean(P, O, local, valid, c, cd, ss, gs, ey, tested_local);
     }
+    flush_tested(O, tested_local);
   }
   __syncthreads();
   tc_fence_after();
@@ -423,7 +465,7 @@ static cudaError_t launch_ts_t(const LaunchTs& L, const CUtensorMap& tm, cudaStr
   if (grid > tiles) grid = tiles;
   const int nbox = (L.wpk * 8 + 127) / 128;
   const int nsub = L.kpad / TS_KS;
-  ts_kernel<N, D0><<<(unsigned)grid, TS_THREADS, smem, st>>>(tm, L.m, nbox, nsub, L.Bimg, b_bytes, *L.P, *L.LM,
+  ts_kernel<N, D0><<<(unsigned)grid, ts_threads(N), smem, st>>>(tm, L.m, nbox, nsub, L.Bimg, b_bytes, *L.P, *L.LM,
                                                              *L.O);
   return cudaGetLastError();
 }

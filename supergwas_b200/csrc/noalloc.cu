@@ -142,6 +142,7 @@ extern "C" int kg_run_device_noalloc(const uint64_t* d_xbits, uint64_t n_kmers, 
     lm.nl[j] = L.nl[j];
     lm.scale[j] = L.scale[j];
   }
+  kg::set_limb_consts(lm);
 
   cudaStream_t st = (cudaStream_t)stream;
   unsigned long long* counters = reinterpret_cast<unsigned long long*>(scratch);

@@ -25,7 +25,20 @@ struct LimbMap {
   int first[KMAX + 1];
   int nl[KMAX + 1];
   double scale[KMAX + 1];
+  // Epilogue constants of the kernels whose accumulators hold -128 * digit
+  // sums (set_limb_consts): for the recombined integer V, biased to the
+  // double 1.5 * 2^52 + V, e = fma(biased, esc, eoff) = V * (-scale / 128)
+  // exactly (both factors are powers of two times integers).
+  double esc[KMAX + 1];   // -scale / 128
+  double eoff[KMAX + 1];  // 1.5 * 2^52 * scale / 128
 };
+
+inline void set_limb_consts(LimbMap& L) {
+  for (int j = 0; j <= KMAX; ++j) {
+    L.esc[j] = -L.scale[j] / 128.0;
+    L.eoff[j] = 6755399441055744.0 * L.scale[j] / 128.0;
+  }
+}
 
 // Device outputs of one launch.
 struct DevOut {
