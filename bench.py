@@ -51,7 +51,7 @@ def measured_peaks():
 
 def profile_traffic():
     """DRAM bytes per k-mer of the split kernel from the committed ncu summary (or None)."""
-    p = os.path.join(ROOT, "profiles", "tc_kernel_n1000_r16.md")
+    p = os.path.join(ROOT, "profiles", "ts_kernel_n1000_r16.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -75,7 +75,7 @@ class Clocks:
         try:
             self.out = tempfile.NamedTemporaryFile("w+", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.dev)], stdout=self.out,
+                                          "-lms", "100", "-i", str(self.dev)], stdout=self.out,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -530,7 +530,7 @@ def run_streaming(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--kmers", type=int, default=0, help="k-mers per GPU (default 2e8)")
