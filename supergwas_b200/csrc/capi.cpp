@@ -86,6 +86,7 @@ void kg_destroy(kg_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   dfree(ctx->dV);
+  dfree(ctx->dT);
   dfree(ctx->dB);
   dfree(ctx->dBts);
   dfree(ctx->dCounters);
@@ -165,6 +166,14 @@ int kg_set_structure_ex(kg_ctx* ctx, const double* U, int n, int k, const double
     KG_CUDA(cudaMemcpy(ctx->dV, V.data(), V.size() * sizeof(double), cudaMemcpyHostToDevice), "copy V");
   }
   if (ctx->opts.precision == KG_PREC_SPLIT_I8) {
+    // byte tables of V for the FP64 refinement of high-chi-square k-mers
+    const int vrows = ctx->nsteps * 128;
+    dfree(ctx->dT);
+    KG_CUDA(cudaMalloc((void**)&ctx->dT, kg::refine_table_len(vrows, ctx->cm) * sizeof(double)),
+            "cudaMalloc(refinement tables)");
+    kg::LaunchTable LT{ctx->dV, vrows, ctx->cm, (unsigned long long)vrows * ctx->cm, 1, ctx->dT};
+    KG_CUDA(kg::launch_refine_table(LT, ctx->stream), "refinement tables");
+    KG_CUDA(cudaStreamSynchronize(ctx->stream), "refinement tables");
     P.refine = 1;
     P.r2_ref = -std::expm1(-kg::REFINE_CHISQ / (double)n);
     e = kg::make_limbs(p, sample_pos, n_row, ctx->opts.limbs_u, ctx->opts.limbs_y, kg::tc_kc(), ctx->limbs);
@@ -292,7 +301,7 @@ int launch_one(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, uint64
   if (e != cudaSuccess) return ctx->cuda_fail(e, "kernel launch");
   ++ctx->launches;
   if (ctx->P.refine) {
-    kg::LaunchFp64 R{dx, m, (int)wpk, ctx->dV, ctx->nsteps, ctx->cm, &ctx->P, &O, ctx->num_sms};
+    kg::LaunchFp64 R{dx, m, (int)wpk, ctx->dV, ctx->nsteps, ctx->cm, &ctx->P, &O, ctx->num_sms, ctx->dT};
     e = kg::launch_refine(R, st);
     if (e != cudaSuccess) return ctx->cuda_fail(e, "refinement launch");
     ++ctx->launches;

@@ -19,6 +19,7 @@ void free_multi(kg_ctx* ctx) {
   dfree(M.dB);
   dfree(M.dPh);
   dfree(M.dV);
+  dfree(M.dT);
   dfree(M.dCounters);
   dfree(M.dTested);
   dfree(M.dHits);
@@ -125,7 +126,7 @@ int enqueue_multi(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, uns
   kg::LaunchMp L{dx, m, (int)wpk, M.kpad, M.NP, M.G, M.xs, M.nb, 0, 0, M.dB, M.dPh, &O, ctx->num_sms};
   cudaError_t e = kg::launch_mp(L, st);
   if (e != cudaSuccess) return ctx->cuda_fail(e, "multi-phenotype kernel launch");
-  kg::LaunchMpRefine R{dx, (int)wpk, M.dV, M.nsteps * 128, M.cm, M.vstride, M.dPh, &O, ctx->num_sms};
+  kg::LaunchMpRefine R{dx, (int)wpk, M.dV, M.nsteps * 128, M.cm, M.vstride, M.dPh, &O, ctx->num_sms, M.dT};
   e = kg::launch_mp_refine(R, st);
   if (e != cudaSuccess) return ctx->cuda_fail(e, "refinement launch");
   ctx->launches += 2;
@@ -324,6 +325,12 @@ int kg_set_phenotypes(kg_ctx* ctx, const kg_pheno* ph, int np, int n_row) {
   KG_CUDA(cudaMemcpy(M.dPh, mph.data(), mph.size() * sizeof(kg::MPheno), cudaMemcpyHostToDevice), "copy");
   KG_CUDA(cudaMalloc((void**)&M.dV, V.size() * sizeof(double)), "cudaMalloc(V)");
   KG_CUDA(cudaMemcpy(M.dV, V.data(), V.size() * sizeof(double), cudaMemcpyHostToDevice), "copy V");
+  const int vrows = M.nsteps * 128;
+  KG_CUDA(cudaMalloc((void**)&M.dT, kg::refine_table_len(vrows, cm) * np * sizeof(double)),
+          "cudaMalloc(refinement tables)");
+  kg::LaunchTable LT{M.dV, vrows, cm, (unsigned long long)M.vstride, np, M.dT};
+  KG_CUDA(kg::launch_refine_table(LT, ctx->stream), "refinement tables");
+  KG_CUDA(cudaStreamSynchronize(ctx->stream), "refinement tables");
   return KG_OK;
 }
 

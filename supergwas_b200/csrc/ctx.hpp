@@ -67,6 +67,7 @@ struct Multi {
   int8_t* dB = nullptr;
   kg::MPheno* dPh = nullptr;
   double* dV = nullptr;
+  double* dT = nullptr;  // byte tables of V (refinement), one block per phenotype
   size_t vstride = 0;
   unsigned long long* dCounters = nullptr;
   unsigned long long* dTested = nullptr;
@@ -113,6 +114,7 @@ struct kg_ctx {
   kg::LimbMap LM{};
   // structure on the device
   double* dV = nullptr;
+  double* dT = nullptr;      // byte tables of V for the split form's FP64 refinement
   int cm = 0, nsteps = 0;
   int8_t* dB = nullptr;      // B image of the smem-A kernel
   int8_t* dBts = nullptr;    // B image of the TMEM-A kernel

@@ -352,4 +352,66 @@ __device__ __forceinline__ void flush_tested(const DevOut& O, uint32_t tested_lo
   if ((threadIdx.x & 31u) == 0 && tot) atomicAdd(O.counters + 0, (unsigned long long)tot);
 }
 
+// ------------------------------------------------- FP64 refinement sums
+// Column sums x . v_j of one packed row from byte tables: T[(g*256 + b)*CM + j]
+// is the sum of column j over the samples of 8-sample group g whose bit is set
+// in b.  Lane l accumulates columns l, l+32, ... over the row's bytes in
+// order, one coalesced table row per byte (instead of one V row per set bit).
+// nwords: words of the row covered by the tables.  Called by a whole warp.
+template <int CM>
+__device__ __forceinline__ void table_row_sums(const uint64_t* __restrict__ row, int nwords,
+                                               const double* __restrict__ T, int lane,
+                                               double (&acc)[(CM + 31) / 32]) {
+  constexpr int JW = (CM + 31) / 32;
+#pragma unroll
+  for (int jj = 0; jj < JW; ++jj) acc[jj] = 0.0;
+  for (int w = 0; w < nwords; ++w) {
+    const uint64_t bits = __ldg(row + w);  // one address for the whole warp
+    const double* Tw = T + (size_t)w * (8 * 256 * CM);
+    double v[8][JW];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      const unsigned b = (unsigned)(bits >> (8 * t)) & 255u;
+      const double* e = Tw + (size_t)(t * 256 + b) * CM;
+#pragma unroll
+      for (int jj = 0; jj < JW; ++jj) {
+        const int j = lane + 32 * jj;
+        v[t][jj] = (j < CM) ? __ldg(e + j) : 0.0;
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+#pragma unroll
+      for (int jj = 0; jj < JW; ++jj) acc[jj] += v[t][jj];
+  }
+}
+
+// From the lane-distributed column sums (column 0 = count, 1..k = U columns,
+// k+1 = y'): c, ss = sum_j (a_j c + e_j)^2 and ey, identical in every lane.
+template <int CM>
+__device__ __forceinline__ void refine_reduce(const EpiParams& P, const double (&acc)[(CM + 31) / 32], int lane,
+                                              int& c, double& ss, double& ey) {
+  constexpr int JW = (CM + 31) / 32;
+  c = (int)__shfl_sync(0xffffffffu, acc[0], 0);
+  const double cd = (double)c;
+  double s2 = 0.0, y = 0.0;
+#pragma unroll
+  for (int jj = 0; jj < JW; ++jj) {
+    const int j = lane + 32 * jj;
+    if (j >= 1 && j <= P.k) {
+      const double sj = P.a[j - 1] * cd + acc[jj];
+      s2 += sj * sj;
+    } else if (j == P.k + 1) {
+      y = acc[jj];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    y += __shfl_xor_sync(0xffffffffu, y, o);
+  }
+  ss = s2;
+  ey = y;
+}
+
 }  // namespace kg

@@ -439,12 +439,12 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
 }
 
 // FP64 recomputation of the candidates of a multi-phenotype launch: one
-// warp per (k-mer, phenotype), the phenotype's FP64 columns at V + p*vstride.
+// warp per (k-mer, phenotype), the phenotype's byte tables at T + p*tstride
+// (lanes own the FP64 columns, one table row per byte of the packed row).
 template <int CM>
-__global__ void __launch_bounds__(256) mp_refine_kernel(const uint64_t* __restrict__ x, int wpk,
-                                                        const double* __restrict__ V, int vrows,
-                                                        unsigned long long vstride, const MPheno* __restrict__ ph,
-                                                        const DevOutMP O) {
+__global__ void __launch_bounds__(256) mp_refine_kernel(const uint64_t* __restrict__ x, int wpk, int nwords,
+                                                        const double* __restrict__ T, unsigned long long tstride,
+                                                        const MPheno* __restrict__ ph, const DevOutMP O) {
   const int lane = threadIdx.x & 31;
   const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x >> 5);
   unsigned long long ncand = O.counters[3];
@@ -455,48 +455,21 @@ __global__ void __launch_bounds__(256) mp_refine_kernel(const uint64_t* __restri
     const unsigned long long gk = ent & MP_KMER_MASK;
     const int p = (int)(ent >> 48);
     const EpiParams& P = ph[p].P;
-    const double* Vp = V + (size_t)p * vstride;
     const uint64_t* row = x + (gk - O.kmer_offset) * (unsigned long long)wpk;
-    double acc[CM];
-#pragma unroll
-    for (int j = 0; j < CM; ++j) acc[j] = 0.0;
-    for (int wi = lane; wi < wpk; wi += 32) {
-      uint64_t bits = __ldg(row + wi);
-      while (bits) {
-        const int b = __ffsll((long long)bits) - 1;
-        bits &= bits - 1;
-        const int smp = wi * 64 + b;
-        if (smp < vrows) {
-          const double* vv = Vp + (size_t)smp * CM;
-#pragma unroll
-          for (int j = 0; j < CM; ++j) acc[j] += vv[j];
-        }
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < CM; ++j)
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+    double acc[(CM + 31) / 32];
+    table_row_sums<CM>(row, nwords, T + (size_t)p * tstride, lane, acc);
+    int c;
+    double ss, ey;
+    refine_reduce<CM>(P, acc, lane, c, ss, ey);
     if (lane == 0) {
-      const int c = (int)acc[0];
-      double ss = 0, ey = 0;
-#pragma unroll
-      for (int j = 1; j < CM; ++j) {
-        if (j <= P.k) {
-          const double sj = P.a[j - 1] * (double)c + acc[j];
-          ss += sj * sj;
-        } else if (j == P.k + 1) {
-          ey = acc[j];
-        }
-      }
       const double xxM = (double)c - ss, xyM = P.b * (double)c + ey;
-      double effect = 0, T = 0, pv = 1;
+      double effect = 0, Tq = 0, pv = 1;
       if (xxM > 1e-12 && P.yyM > 1e-12) {
         double r2 = (xyM * xyM) / (xxM * P.yyM);
         if (r2 < 0) r2 = 0;
         if (r2 >= 1) r2 = 1 - 1e-15;
-        T = (double)P.n * log(1.0 / (1.0 - r2));
-        pv = erfc(sqrt(0.5 * T));
+        Tq = (double)P.n * log(1.0 / (1.0 - r2));
+        pv = erfc(sqrt(0.5 * Tq));
         effect = xyM / (xxM * P.yyM);
       }
       if (pv <= P.p_thresh) {
@@ -508,7 +481,7 @@ __global__ void __launch_bounds__(256) mp_refine_kernel(const uint64_t* __restri
           h.shard = mp_shard(O, gk);
           h.effect = effect;
           h.pval = pv;
-          h.chisq = T;
+          h.chisq = Tq;
           O.hits[slot] = h;
         } else {
           atomicOr(O.counters + 2, (unsigned long long)ERR_HIT_OVERFLOW);
@@ -588,11 +561,18 @@ cudaError_t launch_mp(const LaunchMp& L, cudaStream_t st) {
 
 template <int CM>
 static cudaError_t launch_mp_refine_t(const LaunchMpRefine& L, cudaStream_t st) {
-  mp_refine_kernel<CM><<<(unsigned)(L.num_sms * 4), 256, 0, st>>>(L.x, L.wpk, L.V, L.vrows, L.vstride, L.ph, *L.O);
+  static int per_sm = 0;  // every warp of the grid resident at once (candidates are dealt round-robin)
+  if (per_sm < 1 &&
+      (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mp_refine_kernel<CM>, 256, 0) != cudaSuccess ||
+       per_sm < 1))
+    per_sm = 1;
+  mp_refine_kernel<CM><<<(unsigned)(L.num_sms * per_sm), 256, 0, st>>>(
+      L.x, L.wpk, L.vrows / 64, L.T, (unsigned long long)refine_table_len(L.vrows, L.cm), L.ph, *L.O);
   return cudaGetLastError();
 }
 
 cudaError_t launch_mp_refine(const LaunchMpRefine& L, cudaStream_t st) {
+  if (!L.T) return cudaErrorInvalidValue;
   switch (L.cm) {
     case 8: return launch_mp_refine_t<8>(L, st);
     case 12: return launch_mp_refine_t<12>(L, st);

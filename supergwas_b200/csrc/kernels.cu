@@ -123,12 +123,13 @@ cudaError_t launch_fp64(const LaunchFp64& L, cudaStream_t st) {
 
 // ====================================================== FP64 refinement pass
 // One warp per candidate k-mer (chi-square >= REFINE_CHISQ in the split form):
-// the lanes walk the set bits of the packed row, add the FP64 contraction
-// columns (same layout as the FP64 form), reduce across the warp, and lane 0
-// evaluates compute_hit (src/kgwas.cpp:44-56) and emits the row.
+// the lanes own the FP64 contraction columns (same layout as the FP64 form)
+// and sum them over the row's bytes from the byte tables, one coalesced
+// table row per byte; lane 0 then evaluates compute_hit
+// (src/kgwas.cpp:44-56) in FP64 and emits the row.
 template <int CM>
-__global__ void __launch_bounds__(256) refine_kernel(const uint64_t* __restrict__ x, int wpk,
-                                                     const double* __restrict__ V, int vrows,
+__global__ void __launch_bounds__(256) refine_kernel(const uint64_t* __restrict__ x, int wpk, int nwords,
+                                                     const double* __restrict__ T,
                                                      const __grid_constant__ EpiParams P, const DevOut O) {
   const int lane = threadIdx.x & 31;
   const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x >> 5);
@@ -138,47 +139,21 @@ __global__ void __launch_bounds__(256) refine_kernel(const uint64_t* __restrict_
        w += warps) {
     const unsigned long long g = O.cand[w];
     const uint64_t* row = x + (g - O.kmer_offset) * (unsigned long long)wpk;
-    double acc[CM];
-#pragma unroll
-    for (int j = 0; j < CM; ++j) acc[j] = 0.0;
-    for (int wi = lane; wi < wpk; wi += 32) {
-      uint64_t bits = __ldg(row + wi);
-      while (bits) {
-        const int b = __ffsll((long long)bits) - 1;
-        bits &= bits - 1;
-        const int smp = wi * 64 + b;
-        if (smp < vrows) {
-          const double* v = V + (size_t)smp * CM;
-#pragma unroll
-          for (int j = 0; j < CM; ++j) acc[j] += v[j];
-        }
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < CM; ++j)
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+    double acc[(CM + 31) / 32];
+    table_row_sums<CM>(row, nwords, T, lane, acc);
+    int c;
+    double ss, ey;
+    refine_reduce<CM>(P, acc, lane, c, ss, ey);
     if (lane == 0) {
-      const int c = (int)acc[0];
-      double ss = 0, ey = 0;
-#pragma unroll
-      for (int j = 1; j < CM; ++j) {
-        if (j <= P.k) {
-          const double sj = P.a[j - 1] * (double)c + acc[j];
-          ss += sj * sj;
-        } else if (j == P.k + 1) {
-          ey = acc[j];
-        }
-      }
       const double xxM = (double)c - ss, xyM = P.b * (double)c + ey;
-      double effect = 0, T = 0, p = 1;
+      double effect = 0, Tq = 0, p = 1;
       const double eps = 1e-12;
       if (xxM > eps && P.yyM > eps) {
         double r2 = (xyM * xyM) / (xxM * P.yyM);
         if (r2 < 0) r2 = 0;
         if (r2 >= 1) r2 = 1 - 1e-15;
-        T = (double)P.n * log(1.0 / (1.0 - r2));
-        p = erfc(sqrt(0.5 * T));
+        Tq = (double)P.n * log(1.0 / (1.0 - r2));
+        p = erfc(sqrt(0.5 * Tq));
         effect = xyM / (xxM * P.yyM);
       }
       if (p <= P.p_thresh) {
@@ -188,17 +163,17 @@ __global__ void __launch_bounds__(256) refine_kernel(const uint64_t* __restrict_
           h.kmer = g;
           h.effect = effect;
           h.pval = p;
-          h.chisq = T;
+          h.chisq = Tq;
           O.hits[slot] = h;
         } else {
           atomicOr(O.counters + 2, (unsigned long long)ERR_HIT_OVERFLOW);
         }
       }
       if (O.tested) {
-        O.chisq[g] = T;
+        O.chisq[g] = Tq;
         O.pval[g] = p;
         O.effect[g] = effect;
-        O.mlog10p[g] = mlog10_sf(T);
+        O.mlog10p[g] = mlog10_sf(Tq);
         O.xxM[g] = xxM;
         O.xyM[g] = xyM;
       }
@@ -208,12 +183,17 @@ __global__ void __launch_bounds__(256) refine_kernel(const uint64_t* __restrict_
 
 template <int CM>
 static cudaError_t launch_refine_t(const LaunchFp64& L, cudaStream_t st) {
-  const unsigned grid = (unsigned)(L.num_sms * 4);
-  refine_kernel<CM><<<grid, 256, 0, st>>>(L.x, L.wpk, L.V, L.nsteps * F64_SCH, *L.P, *L.O);
+  static int per_sm = 0;  // every warp of the grid resident at once (candidates are dealt round-robin)
+  if (per_sm < 1 &&
+      (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, refine_kernel<CM>, 256, 0) != cudaSuccess || per_sm < 1))
+    per_sm = 1;
+  const unsigned grid = (unsigned)(L.num_sms * per_sm);
+  refine_kernel<CM><<<grid, 256, 0, st>>>(L.x, L.wpk, L.nsteps * F64_SCH / 64, L.T, *L.P, *L.O);
   return cudaGetLastError();
 }
 
 cudaError_t launch_refine(const LaunchFp64& L, cudaStream_t st) {
+  if (!L.T) return cudaErrorInvalidValue;
   switch (L.cm) {
     case 8: return launch_refine_t<8>(L, st);
     case 12: return launch_refine_t<12>(L, st);
@@ -227,6 +207,40 @@ cudaError_t launch_refine(const LaunchFp64& L, cudaStream_t st) {
     case 68: return launch_refine_t<68>(L, st);
     default: return cudaErrorInvalidValue;
   }
+}
+
+// Byte tables: one thread per (block, group, byte value, column); the entry
+// adds the group's set samples in ascending order.
+__global__ void __launch_bounds__(256) refine_table_kernel(const double* __restrict__ V, int cm,
+                                                           unsigned long long vstride, unsigned long long total,
+                                                           unsigned long long per_block, double* __restrict__ T) {
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long blk = i / per_block;
+    const unsigned long long r = i - blk * per_block;
+    const int j = (int)(r % (unsigned)cm);
+    const unsigned long long gb = r / (unsigned)cm;
+    const unsigned b = (unsigned)(gb & 255u);
+    const unsigned long long grp = gb >> 8;
+    const double* v = V + blk * vstride + grp * 8ull * (unsigned)cm + j;
+    double s = 0.0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if ((b >> t) & 1u) s += v[(size_t)t * cm];
+    T[i] = s;
+  }
+}
+
+size_t refine_table_len(int vrows, int cm) { return (size_t)(vrows / 8) * 256 * (size_t)cm; }
+
+cudaError_t launch_refine_table(const LaunchTable& L, cudaStream_t st) {
+  if (L.vrows % 128 || L.cm <= 0 || L.nblocks <= 0 || !L.V || !L.T) return cudaErrorInvalidValue;
+  const unsigned long long tlen = refine_table_len(L.vrows, L.cm);
+  const unsigned long long total = tlen * (unsigned long long)L.nblocks;
+  unsigned long long blocks = (total + 255) / 256;
+  if (blocks > 65535ull * 16) blocks = 65535ull * 16;
+  refine_table_kernel<<<(unsigned)blocks, 256, 0, st>>>(L.V, L.cm, L.vstride, total, tlen, L.T);
+  return cudaGetLastError();
 }
 
 // ============================================== tcgen05 kind::i8, A from SMEM

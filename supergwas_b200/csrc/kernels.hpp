@@ -15,6 +15,7 @@ struct LaunchFp64 {
   const EpiParams* P;
   const DevOut* O;
   int num_sms;
+  const double* T = nullptr;  // refinement byte tables of V (refine_table_len doubles; device)
 };
 
 struct LaunchTc {
@@ -32,8 +33,22 @@ struct LaunchTc {
 int fp64_cm(int C);           // padded column count for C contraction columns (-1: too many)
 int fp64_steps(int n);        // 128-sample steps covering n samples
 cudaError_t launch_fp64(const LaunchFp64& L, cudaStream_t st);
-// FP64 recomputation of the split form's refinement candidates (same V layout).
+// FP64 recomputation of the split form's refinement candidates from the
+// byte tables of V (LaunchFp64::T).
 cudaError_t launch_refine(const LaunchFp64& L, cudaStream_t st);
+
+// Byte tables of the FP64 columns, one block per phenotype: for the 8-sample
+// group g of a packed row and a byte value b, entry (g*256 + b)*cm + j is the
+// sum of column j of V over the samples of g whose bit is set in b.
+struct LaunchTable {
+  const double* V;            // nblocks blocks of vrows x cm FP64 (vstride doubles apart)
+  int vrows, cm;              // vrows a multiple of 128
+  unsigned long long vstride;
+  int nblocks;
+  double* T;                  // nblocks blocks of refine_table_len(vrows, cm) doubles
+};
+size_t refine_table_len(int vrows, int cm);
+cudaError_t launch_refine_table(const LaunchTable& L, cudaStream_t st);
 
 struct LaunchTs {
   const uint64_t* x;          // packed rows (device), 16-byte aligned
@@ -75,6 +90,7 @@ struct LaunchMpRefine {
   const MPheno* ph;
   const DevOutMP* O;
   int num_sms;
+  const double* T = nullptr;  // byte tables of V, refine_table_len(vrows, cm) doubles per phenotype
 };
 bool mp_supported(int NP, int wpk);
 size_t mp_smem_bytes(int nbox, int xs, int nb, int N);
