@@ -102,9 +102,10 @@ class Clocks:
         mx = max(float(r[2]) for r in rows)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
-        load = [s for s, r in zip(sm, rows) if float(r[3]) > 200.0] or sm
+        pw = [float(r[3]) for r in rows]
+        load = [s for s, w in zip(sm, pw) if w > 200.0] or sm
         return {"sm_mhz": statistics.median(load), "sm_max_mhz": mx, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "power_w_median": statistics.median(pw), "power_w_max": max(pw)}
 
 
 # ------------------------------------------------------------ CPU baseline

@@ -10,9 +10,9 @@
 //   warps 8-15  unpack, two groups of four taking super-stages in turn (one
 //               group for N > 80, so that the epilogue keeps its registers): read
 //               128 samples of a packed row from the TMA-filled shared tile
-//               and write them as int8 (0 / -128) straight into a TMEM A slot
-//               with tcgen05.st -- the unpacked operand never touches shared
-//               memory;
+//               and write them as int8 (0 / -128, or 0 / 64 against -2x the
+//               B digits) straight into a TMEM A slot with tcgen05.st -- the
+//               unpacked operand never touches shared memory;
 //   warp 16     producer (12 for N > 80): one 2-D TMA load (128 rows x 128 bytes, 128-byte
 //               swizzle, no multicast) per 1024 samples of a 128-k-mer tile;
 //   warp 17     MMA (13 for N > 80): tcgen05.mma kind::i8, A from TMEM, B (the int8 limbs of
@@ -21,8 +21,9 @@
 // Tile = 128 k-mers (M), N = 16..128 limb columns.
 //
 // The MMA-issuing thread is the critical path: on B200 a kind::i8 M=128
-// N=64 MMA occupies the tensor pipe ~47 cycles, and every barrier test,
-// commit or runtime division between MMAs adds its latency on top.  So the
+// N=64 K=32 MMA occupies the tensor pipe 32 cycles (16384 int8 ops per SM
+// cycle), and every barrier test, commit or runtime division between MMAs
+// adds its latency on top.  So the
 // A operand moves in super-stages of 512 samples (4 sub-stages of 128
 // samples = 128 TMEM columns = 16 MMAs) with one barrier wait and one
 // commit each, and every ring index is a compile-time-bounded counter.
@@ -92,6 +93,20 @@ __device__ __forceinline__ void tc_st32(uint32_t taddr, const uint32_t (&r)[32])
       "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]),
       "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
       : "memory");
+}
+
+// 128 packed samples (four 32-bit words) -> 32 TMEM columns of int8 A
+// operand: column 8q+jj holds, in byte t, sample 32q + 8t + 7 - jj as -128 x
+// (jj even) or 64 x (jj odd).  make_b_image_ts lays B out to match.
+__device__ __forceinline__ void unpack_stage(const uint32_t (&w)[4], uint32_t (&o)[32]) {
+#pragma unroll
+  for (int qq = 0; qq < 4; ++qq)
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const uint32_t u = w[qq] * (1u << (2 * h));
+      o[qq * 8 + 2 * h] = u & 0x80808080u;
+      o[qq * 8 + 2 * h + 1] = u & 0x40404040u;
+    }
 }
 
 // Bounded wait that also gives up when another role has aborted.  The first
@@ -311,10 +326,12 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
           const uint32_t a_t = tmem + lane_base + A0 + ar.slot * 128;
           const int c0 = kc - bx * (TS_BOX / TS_KS);
           // 16 bytes (128 samples) of row r per sub-stage; 128-byte swizzle:
-          // chunk c of row r sits at c ^ (r % 8).  Byte t of column 8qq+j =
-          // bit 8t+j of word qq, moved to the byte's sign bit (0 or -128); the
-          // shift is a multiply so that it issues on the FMA pipe and the mask
-          // on the ALU pipe.
+          // chunk c of row r sits at c ^ (r % 8).  Column 8qq+jj of a stage =
+          // word qq shifted left by 2*(jj/2), masked to bit 7 (jj even: byte t
+          // holds sample 8t+7-jj as 0 / -128) or bit 6 (jj odd: 0 / 64; the B
+          // image holds -2 V there), so one shift serves two columns.  The
+          // shift is a multiply so that it issues on the FMA pipe and the
+          // masks on the ALU pipe.
           if (ke - kc == TS_SUPER) {
             uint32_t w[TS_SUPER][4];
 #pragma unroll
@@ -325,10 +342,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
 #pragma unroll
             for (int sub = 0; sub < TS_SUPER; ++sub) {
               uint32_t o[32];
-#pragma unroll
-              for (int qq = 0; qq < 4; ++qq)
-#pragma unroll
-                for (int j = 0; j < 8; ++j) o[qq * 8 + j] = (w[sub][qq] * (1u << (7 - j))) & 0x80808080u;
+              unpack_stage(w[sub], o);
               tc_st32(a_t + sub * 32, o);
             }
           } else {
@@ -339,10 +353,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
                            : "r"(xrow + (((c0 + sub) ^ (r & 7)) << 4)));
               const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
               uint32_t o[32];
-#pragma unroll
-              for (int qq = 0; qq < 4; ++qq)
-#pragma unroll
-                for (int j = 0; j < 8; ++j) o[qq * 8 + j] = (w4[qq] * (1u << (7 - j))) & 0x80808080u;
+              unpack_stage(w4, o);
               tc_st32(a_t + sub * 32, o);
             }
           }
@@ -393,11 +404,13 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
       //   e = V * (-scale/128) = v * scale, exact (LimbMap esc/eoff);
       //   y':       |V| < 2^57, so v = -V >> 7 (exact) first.
       // The values equal those of the smem-A kernel bit for bit.
+      // Each partial sum below is one 32 x 32 -> 64-bit multiply-add (the
+      // limb sums are int32, |d| <= 2^24).
       const int c = (-(int)d[0]) >> 7;
       const double cd = i2d_exact(c);
-      long long Vy = (int)d[1];
+      long long Vy = (long long)(int)d[1 + TS_LY - 1];
 #pragma unroll
-      for (int l = 1; l < TS_LY; ++l) Vy = Vy * 256 + (int)d[1 + l];
+      for (int l = 1; l < TS_LY; ++l) Vy += (long long)(int)d[TS_LY - l] * (1ll << (8 * l));
       const double sy = LM.scale[P.k];
       const double ey = fma(magic_raw((-Vy) >> 7), sy, -MAGIC_BIAS * sy);
       double ss = 0, gs = 0;
@@ -412,10 +425,11 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
       for (int jj = 0; jj < KU_MAX; ++jj) {
         const int j = jj + (DROP0 ? 1 : 0);
         const int o = 1 + TS_LY + TS_LU * jj;
-        long long V = (int)d[o];
+        // biased: 1.5 * 2^52 + V as a bit pattern, V = sum_l 256^(L-1-l) d_l
+        long long Vb = (long long)(int)d[o + TS_LU - 1] + (long long)0x4338000000000000LL;
 #pragma unroll
-        for (int l = 1; l < TS_LU; ++l) V = V * 256 + (int)d[o + l];
-        const double e = fma(magic_raw(V), LM.esc[j], LM.eoff[j]);
+        for (int l = 1; l < TS_LU; ++l) Vb += (long long)(int)d[o + TS_LU - 1 - l] * (1ll << (8 * l));
+        const double e = fma(__longlong_as_double(Vb), LM.esc[j], LM.eoff[j]);
         const double sj = fma(P.a[j], cd, e);
         ss = fma(sj, sj, ss);
         gs = fma(P.g[j], e, gs);

@@ -130,6 +130,31 @@ def test_prep_algebra_matches_oracle(split):
             assert ml[msk].max() <= 1e-11
 
 
+def test_tmem_b_image_matches_unpack():
+    """make_b_image_ts lays B out for the A bytes the TMEM kernel's unpack
+    forms (two masks per shift, -2 V on the 64 x columns): recombined limb
+    sums equal -128 * x . V for every column, with no int32 overflow."""
+    L = emu_lib()
+    L.ts_image_check.restype = ctypes.c_int64
+    dp = ctypes.POINTER(ctypes.c_double)
+    for (n, m, S, r, seed) in [(1000, 600, 8, 16, 5), (61, 400, 3, 3, 6), (300, 300, 4, 6, 7)]:
+        ds = synth.simulate(n=n, m=m, S=S, r=r, n_causal=10, missing=0.05, seed=seed)
+        X = np.ascontiguousarray(ds.packed_overlap())
+        Uc = np.ascontiguousarray(np.asarray(ds.U).T)
+        y = np.ascontiguousarray(ds.y, dtype=np.float64)
+        bad = L.ts_image_check(Uc.ctypes.data_as(dp), ds.n, ds.U.shape[1], y.ctypes.data_as(dp),
+                               X.ctypes.data_as(ctypes.c_void_p), ctypes.c_int64(X.shape[0]), X.shape[1])
+        assert bad == 0, (n, bad)
+    # all-ones rows: largest limb sums
+    ds = synth.simulate(n=1000, m=50, S=8, r=16, n_causal=5, missing=0.0, seed=8)
+    X = np.full_like(ds.packed_overlap(), np.uint64(0xFFFFFFFFFFFFFFFF))
+    Uc = np.ascontiguousarray(np.asarray(ds.U).T)
+    y = np.ascontiguousarray(ds.y, dtype=np.float64)
+    bad = L.ts_image_check(Uc.ctypes.data_as(dp), ds.n, ds.U.shape[1], y.ctypes.data_as(dp),
+                           X.ctypes.data_as(ctypes.c_void_p), ctypes.c_int64(X.shape[0]), X.shape[1])
+    assert bad == 0
+
+
 def test_prep_general_U_without_intercept():
     """U that does not contain the constant vector (no intercept column)."""
     fx = H.load_fixture("edge")
