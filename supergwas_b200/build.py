@@ -12,6 +12,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
@@ -20,9 +21,10 @@ LIB_DIR = os.path.join(PKG, "lib")
 BIN_DIR = os.path.join(PKG, "bin")
 LIB = os.path.join(LIB_DIR, "libkgwas_cuda.so")
 CLI = os.path.join(BIN_DIR, "kgwas")
+OBJ_DIR = os.path.join(PKG, "_build")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-LIB_SOURCES = ["kernels.cu", "kernel_ts.cu", "kernel_mp.cu", "noalloc.cu", "capi.cpp", "capi_multi.cpp", "prep.cpp"]
+LIB_SOURCES = ["kernels.cu", "kernel_ts.cu", "kernel_mp.cu", "kernel_mpb.cu", "noalloc.cu", "capi.cpp", "capi_multi.cpp", "prep.cpp"]
 CLI_SOURCES = ["kgwas_main.cpp", "kgwas_io.cpp"]
 
 
@@ -59,17 +61,23 @@ def run(cmd, verbose=False):
 
 
 def build_lib(force=False, verbose=False, ptxas_verbose=False) -> str:
+    """Compile every source to an object in parallel, then link the shared library."""
     deps = _deps(LIB_SOURCES)
     if not force and _newer(LIB, deps):
         return LIB
     os.makedirs(LIB_DIR, exist_ok=True)
-    cmd = [nvcc(), *ARCH, "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3",
-           "-shared", "-o", LIB, *[os.path.join(CSRC, s) for s in LIB_SOURCES]]
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    base = [nvcc(), *ARCH, "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3"]
     if ptxas_verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    r = run(cmd, verbose)
+        base.append("-Xptxas=-v")
+    objs = [os.path.join(OBJ_DIR, os.path.splitext(s)[0] + ".o") for s in LIB_SOURCES]
+    cmds = [base + ["-c", os.path.join(CSRC, s), "-o", o] for s, o in zip(LIB_SOURCES, objs)]
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        results = list(ex.map(lambda c: run(c, verbose), cmds))
     if ptxas_verbose:
-        sys.stderr.write(r.stderr)
+        for r in results:
+            sys.stderr.write(r.stderr)
+    run([nvcc(), *ARCH, "-shared", "-o", LIB, *objs], verbose)
     return LIB
 
 

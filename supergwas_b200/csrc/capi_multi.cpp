@@ -43,7 +43,7 @@ void drop_graph(Multi& M) {
 // Resident x tiles and B ring stages that fit the shared memory.
 void pick_shape(Multi& M, int nbox, int xs_pref, int nb_pref) {
   const size_t budget = 220 * 1024;
-  const int N = (128 / M.NP) * M.NP;
+  const int N = M.PPG * M.NP;
   int xs = xs_pref, nb = nb_pref;
   while (xs > 1 && kg::mp_smem_bytes(nbox, xs, 2, N) > budget) --xs;
   while (nb > 2 && kg::mp_smem_bytes(nbox, xs, nb, N) > budget) --nb;
@@ -123,8 +123,22 @@ int enqueue_multi(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, uns
   if (m == 0) return KG_OK;
   kg::DevOutMP O = dev_out(ctx, offset);
   KG_CUDA(cudaMemsetAsync(M.dCounters + 3, 0, sizeof(unsigned long long), st), "memset");
-  kg::LaunchMp L{dx, m, (int)wpk, M.kpad, M.NP, M.G, M.xs, M.nb, 0, 0, M.dB, M.dPh, &O, ctx->num_sms};
-  cudaError_t e = kg::launch_mp(L, st);
+  cudaError_t e;
+  if (M.stationary) {
+    // tile-iterations per block: the block's packed rows (every CTA's) stay in L2
+    // across the G passes
+    const unsigned long long tiles = (m + 127) / 128;
+    const unsigned long long grid = std::min<unsigned long long>(tiles, (unsigned long long)ctx->num_sms);
+    const unsigned long long tile_bytes = 128ull * wpk * 8;
+    unsigned long long bt = (48ull << 20) / std::max<unsigned long long>(1, grid * tile_bytes);
+    if (const char* v = std::getenv("KG_MP_BT")) bt = (unsigned long long)std::max(1, std::atoi(v));
+    bt = std::max<unsigned long long>(1, std::min<unsigned long long>(bt, 1024));
+    kg::LaunchMpb L{dx, m, (int)wpk, M.kpad, M.NP, M.PPG, M.G, (int)bt, M.dB, M.dPh, &O, ctx->num_sms};
+    e = kg::launch_mpb(L, st);
+  } else {
+    kg::LaunchMp L{dx, m, (int)wpk, M.kpad, M.NP, M.PPG, M.G, M.xs, M.nb, 0, 0, M.dB, M.dPh, &O, ctx->num_sms};
+    e = kg::launch_mp(L, st);
+  }
   if (e != cudaSuccess) return ctx->cuda_fail(e, "multi-phenotype kernel launch");
   kg::LaunchMpRefine R{dx, (int)wpk, M.dV, M.nsteps * 128, M.cm, M.vstride, M.dPh, &O, ctx->num_sms, M.dT};
   e = kg::launch_mp_refine(R, st);
@@ -146,6 +160,11 @@ int autotune(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, cudaStre
   Multi& M = ctx->mp;
   const int nbox = ((int)wpk * 8 + 127) / 128;
   if (M.tuned && M.tuned_nbox == nbox) return KG_OK;
+  if (M.stationary) {  // the B-stationary kernel has no ring shape to choose
+    M.tuned = true;
+    M.tuned_nbox = nbox;
+    return KG_OK;
+  }
   if (const char* v = std::getenv("KG_MP_SHAPE")) {  // "xs,nb": fixed shape, no tuning
     int xs = 1, nb = 4;
     if (std::sscanf(v, "%d,%d", &xs, &nb) == 2) {
@@ -219,7 +238,7 @@ int check_multi(kg_ctx* ctx, const void* x, uint64_t m, uint32_t wpk) {
   if (m > 0 && !x) return ctx->fail(KG_ERR_INVALID, "xbits is NULL");
   if (wpk == 0 || (wpk & 1u)) return ctx->fail(KG_ERR_INVALID, "words_per_kmer must be even and > 0");
   if ((uint64_t)wpk * 64 < (uint64_t)M.n_row) return ctx->fail(KG_ERR_INVALID, "words_per_kmer*64 < samples per row");
-  if (!kg::mp_supported(M.NP, (int)wpk))
+  if (!kg::mp_supported(M.NP, M.PPG, (int)wpk))
     return ctx->fail(KG_ERR_UNSUPPORTED, "rows must be at least 128 bytes (pad words_per_kmer to 16)");
   if (m >= (1ull << 48)) return ctx->fail(KG_ERR_UNSUPPORTED, "more than 2^48 k-mers in one call");
   return KG_OK;
@@ -259,32 +278,41 @@ int kg_set_phenotypes(kg_ctx* ctx, const kg_pheno* ph, int np, int n_row) {
     NP = std::max(NP, limbs[p].N);
   }
   if (NP > 128) return ctx->fail(KG_ERR_UNSUPPORTED, "a phenotype needs more than 128 limb columns (r too large)");
-  const int PPG = 128 / NP, N = PPG * NP, G = (np + PPG - 1) / PPG;
-  const int kpad = limbs[0].Kpad, nchunk = kpad / 128;
+  // Phenotypes per group: a power of two with NP * PPG <= 128.  The
+  // B-stationary kernel needs the group image (kpad x NP*PPG) and the x ring
+  // in shared memory: take the widest group that fits; if none does, the
+  // streamed-B kernel runs the widest group.
+  const int kpad = limbs[0].Kpad;
+  int PPG = 1;
+  while (PPG * 2 * NP <= 128) PPG *= 2;
+  bool stationary = false;
+  if (!std::getenv("KG_MP_STREAMED"))
+    for (int q = PPG; q >= 1 && !stationary; q /= 2)
+      if (kg::mpb_supported(NP, q, kpad, 16)) {
+        PPG = q;
+        stationary = true;
+      }
+  const int N = PPG * NP, G = (np + PPG - 1) / PPG;
   M.np = np;
   M.n_row = n_row;
   M.NP = NP;
+  M.PPG = PPG;
+  M.stationary = stationary;
   M.G = G;
   M.kpad = kpad;
-  // B image: group gi, chunk kc at (gi*nchunk + kc)*128*N; phenotype slot pp at
-  // columns [pp*NP, pp*NP + its N); K permuted inside each 128-sample chunk
-  // exactly as make_b_image_ts does.
-  std::vector<int8_t> img((size_t)G * nchunk * 128 * N, 0);
-  for (int p = 0; p < np; ++p) {
-    const kg::LimbCols& L = limbs[p];
-    const int gi = p / PPG, pp = p % PPG;
-    if (L.first[prep[p].k] != 1 || L.nl[prep[p].k] != 5)
-      return ctx->fail(KG_ERR_INVALID, "unexpected limb layout");
-    for (int kap = 0; kap < kpad; ++kap) {
-      const int kc = kap / 128, w = kap % 128, c = w / 4, t = w % 4, q4 = c / 8, j = c % 8;
-      const int i = 128 * kc + 32 * q4 + 8 * t + j;
-      const size_t cb = ((size_t)gi * nchunk + kc) * 128 * N;
-      for (int col = 0; col < L.N; ++col) {
-        const int cc = pp * NP + col;
-        img[cb + (size_t)(w / 16) * (N * 16) + (size_t)(cc / 8) * 128 + (size_t)(cc % 8) * 16 + (w % 16)] =
-            L.vals[(size_t)col * L.Kpad + i];
-      }
+  // B image: group gi at gi*kpad*N in the make_b_image_ts layout (the
+  // streamed-B kernel reads it 128 samples at a time), phenotype slot pp at
+  // columns [pp*NP, pp*NP + its N).
+  std::vector<int8_t> img((size_t)G * kpad * N, 0);
+  for (int gi = 0; gi < G; ++gi) {
+    std::vector<int8_t> gimg((size_t)kpad * N, 0);
+    for (int pp = 0; pp < PPG && gi * PPG + pp < np; ++pp) {
+      const int p = gi * PPG + pp;
+      if (limbs[p].first[prep[p].k] != 1 || limbs[p].nl[prep[p].k] != 5 || limbs[p].Kpad != kpad)
+        return ctx->fail(KG_ERR_INVALID, "unexpected limb layout");
+      kg::put_b_image_ts(limbs[p], pp * NP, N, gimg);
     }
+    std::copy(gimg.begin(), gimg.end(), img.begin() + (size_t)gi * kpad * N);
   }
   std::vector<kg::MPheno> mph(np);
   int cm = 8;

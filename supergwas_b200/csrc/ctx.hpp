@@ -64,6 +64,8 @@ inline void fill_epi(kg::EpiParams& P, const kg::Prepared& p, const kg_opts& o, 
 // State of the many-phenotype path.
 struct Multi {
   int np = 0, n_row = 0, NP = 0, G = 0, kpad = 0, cm = 0, nsteps = 0;
+  int PPG = 1;          // phenotypes per group (one MMA of NP * PPG columns)
+  bool stationary = false;  // the group image fits in shared memory: kernel_mpb.cu
   int8_t* dB = nullptr;
   kg::MPheno* dPh = nullptr;
   double* dV = nullptr;

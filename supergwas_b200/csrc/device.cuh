@@ -158,6 +158,73 @@ __host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
   return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
+// ------------------------------------------- TMEM-A kernels (shared parts)
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const void* tmap, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"(tmap), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_st32(uint32_t taddr, const uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+      "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]),
+      "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]),
+      "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
+      : "memory");
+}
+
+// 128 packed samples (four 32-bit words) -> 32 TMEM columns of int8 A
+// operand: column 8q+jj holds, in byte t, sample 32q + 8t + 7 - jj as -128 x
+// (jj even) or 64 x (jj odd).  make_b_image_ts lays B out to match.
+__device__ __forceinline__ void unpack_stage(const uint32_t (&w)[4], uint32_t (&o)[32]) {
+#pragma unroll
+  for (int qq = 0; qq < 4; ++qq)
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const uint32_t u = w[qq] * (1u << (2 * h));
+      o[qq * 8 + 2 * h] = u & 0x80808080u;
+      o[qq * 8 + 2 * h + 1] = u & 0x40404040u;
+    }
+}
+
+// Bounded wait that also gives up when another role has aborted.  The first
+// test is inline (the common case: the phase is already complete); the
+// abort flag and the clock are read only every 16 failed tests.
+__device__ __forceinline__ bool wait_or_abort(uint32_t bar, uint32_t parity, volatile int* abort,
+                                        unsigned long long* counters, unsigned code) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = gtimer_ns();
+  for (uint32_t it = 1;; ++it) {
+    if (mbar_try(bar, parity)) return true;
+    if ((it & 15u) == 0) {
+      if (*abort) return false;
+      if (gtimer_ns() - t0 > WAIT_LIMIT_NS) {
+        atomicOr(counters + 2, (unsigned long long)code);
+        *abort = 1;
+        return false;
+      }
+    }
+  }
+}
+
+// Ring position: slot index and phase parity, advanced without division.
+template <int NS>
+struct Ring {
+  uint32_t slot = 0, phase = 0, used = 0;  // used: laps completed (0 = first)
+  __device__ __forceinline__ void next() {
+    if (++slot == (uint32_t)NS) {
+      slot = 0;
+      phase ^= 1u;
+      used = 1;
+    }
+  }
+};
+
 // ---------------------------------------------------------------- epilogue
 // -log10 erfc(z) without underflow (log-domain tail through erfcx).
 __device__ __forceinline__ double mlog10_sf(double T) {
@@ -412,6 +479,107 @@ __device__ __forceinline__ void refine_reduce(const EpiParams& P, const double (
   }
   ss = s2;
   ey = y;
+}
+
+// ------------------------------------------------ many-phenotype helpers
+// Shard of a global k-mer index (shard_start ascending, shard_start[0] = 0).
+__device__ __forceinline__ int mp_shard(const DevOutMP& O, unsigned long long gk) {
+  int lo = 0, hi = O.n_shards - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (O.shard_start[mid] <= gk) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Statistic of one (k-mer, phenotype) from the exact integer sums, as the
+// division-free screen of finish_kmer_fast; writes the outcome flags.
+__device__ __forceinline__ void mp_eval(const EpiParams& P, bool valid, int c, double ss, double gs, double ey,
+                                        bool& tested, bool& hit, bool& cand, double& T, double& p, double& effect) {
+  const int n = P.n;
+  tested = valid && c > 0 && c < n && !(P.ynorm < 1e-12);
+  if (tested && P.corr_thr > 0.0) {
+    const double xcn2 = (double)c * (double)(n - c) / (double)n;
+    const double xyc = ey + gs + P.kappa * (double)c;
+    tested = xyc * xyc >= P.thr2_ynorm2 * xcn2;
+  }
+  hit = cand = false;
+  T = 0;
+  p = 1;
+  effect = 0;
+  if (!tested) return;
+  const double xxM = (double)c - ss, xyM = P.b * (double)c + ey;
+  const double eps = 1e-12;
+  if (!(xxM > eps && P.yyM > eps)) {
+    hit = p <= P.p_thresh;
+    return;
+  }
+  const double q = xyM * xyM, den = xxM * P.yyM;
+  if (P.refine && q >= P.r2_ref * den) {
+    cand = true;
+  } else if (q >= P.r2_cand * den) {
+    double r2 = q / den;
+    if (r2 < 0) r2 = 0;
+    if (r2 >= 1) r2 = 1 - 1e-15;
+    T = (double)n * log(1.0 / (1.0 - r2));
+    p = erfc(sqrt(0.5 * T));
+    effect = xyM / den;
+    hit = p <= P.p_thresh;
+  }
+}
+
+// Warp-aggregated hit records and FP64 refinement candidates (k-mer |
+// phenotype << 48) of one (k-mer, phenotype) per lane.  mp_emit adds the
+// tested count of (shard, phenotype) with one atomic per shard present in the
+// warp (match = the lanes of this lane's shard, leader = the lowest of them).
+// All 32 lanes of the warp must call them.
+__device__ __forceinline__ void mp_emit_rare(const DevOutMP& O, int p, unsigned long long gk, int shard, bool hit,
+                                             bool cand, double T, double pv, double effect) {
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned hm = __ballot_sync(0xffffffffu, hit);
+  if (hm) {
+    unsigned long long hb = 0;
+    const int hl = __ffs(hm) - 1;
+    if ((int)lane == hl) hb = atomicAdd(O.counters + 1, (unsigned long long)__popc(hm));
+    hb = __shfl_sync(0xffffffffu, hb, hl);
+    if (hit) {
+      const unsigned long long slot = hb + __popc(hm & ((1u << lane) - 1u));
+      if (slot < O.hit_cap) {
+        kg_phit hrec;
+        hrec.kmer = gk;
+        hrec.pheno = p;
+        hrec.shard = shard;
+        hrec.effect = effect;
+        hrec.pval = pv;
+        hrec.chisq = T;
+        O.hits[slot] = hrec;
+      } else {
+        atomicOr(O.counters + 2, (unsigned long long)ERR_HIT_OVERFLOW);
+      }
+    }
+  }
+  const unsigned cm = __ballot_sync(0xffffffffu, cand);
+  if (cm) {
+    unsigned long long cb = 0;
+    const int cl = __ffs(cm) - 1;
+    if ((int)lane == cl) cb = atomicAdd(O.counters + 3, (unsigned long long)__popc(cm));
+    cb = __shfl_sync(0xffffffffu, cb, cl);
+    if (cand) {
+      const unsigned long long slot = cb + __popc(cm & ((1u << lane) - 1u));
+      if (slot < O.cand_cap) O.cand[slot] = gk | ((unsigned long long)p << 48);
+      else atomicOr(O.counters + 2, (unsigned long long)ERR_CAND_OVERFLOW);
+    }
+  }
+}
+
+__device__ __forceinline__ void mp_emit(const DevOutMP& O, int p, unsigned long long gk, int shard, unsigned match,
+                                        bool leader, bool tested, bool hit, bool cand, double T, double pv,
+                                        double effect) {
+  const unsigned tm = __ballot_sync(0xffffffffu, tested);
+  if (leader && (tm & match))
+    atomicAdd(O.tested + (size_t)shard * O.n_pheno + p, (unsigned long long)__popc(tm & match));
+  mp_emit_rare(O, p, gk, shard, hit, cand, T, pv, effect);
 }
 
 }  // namespace kg

@@ -56,94 +56,13 @@ __host__ __device__ inline MpSmem mp_smem(int nbox, int xs, int nb, int N) {
   return L;
 }
 
-__device__ __forceinline__ void mp_tma_2d(uint32_t dst, const void* tmap, int x, int y, uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          dst),
-      "l"(tmap), "r"(x), "r"(y), "r"(bar)
-      : "memory");
-}
-
-__device__ __forceinline__ void mp_st32(uint32_t taddr, const uint32_t (&r)[32]) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
-      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
-      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
-      "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]),
-      "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]),
-      "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
-      : "memory");
-}
-
-__device__ __forceinline__ bool mp_wait(uint32_t bar, uint32_t parity, volatile int* abort,
-                                        unsigned long long* counters, unsigned code) {
-  if (mbar_try(bar, parity)) return true;
-  const unsigned long long t0 = gtimer_ns();
-  for (;;) {
-    if (mbar_try(bar, parity)) return true;
-    if (*abort) return false;
-    if (gtimer_ns() - t0 > WAIT_LIMIT_NS) {
-      atomicOr(counters + 2, (unsigned long long)code);
-      *abort = 1;
-      return false;
-    }
-  }
-}
-
-// Shard of a global k-mer index (shard_start ascending, shard_start[0] = 0).
-__device__ __forceinline__ int mp_shard(const DevOutMP& O, unsigned long long gk) {
-  int lo = 0, hi = O.n_shards - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (O.shard_start[mid] <= gk) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
-// Statistic of one (k-mer, phenotype) from the exact integer sums, as the
-// division-free screen of finish_kmer_fast; writes the outcome flags.
-__device__ __forceinline__ void mp_eval(const EpiParams& P, bool valid, int c, double ss, double gs, double ey,
-                                        bool& tested, bool& hit, bool& cand, double& T, double& p, double& effect) {
-  const int n = P.n;
-  tested = valid && c > 0 && c < n && !(P.ynorm < 1e-12);
-  if (tested && P.corr_thr > 0.0) {
-    const double xcn2 = (double)c * (double)(n - c) / (double)n;
-    const double xyc = ey + gs + P.kappa * (double)c;
-    tested = xyc * xyc >= P.thr2_ynorm2 * xcn2;
-  }
-  hit = cand = false;
-  T = 0;
-  p = 1;
-  effect = 0;
-  if (!tested) return;
-  const double xxM = (double)c - ss, xyM = P.b * (double)c + ey;
-  const double eps = 1e-12;
-  if (!(xxM > eps && P.yyM > eps)) {
-    hit = p <= P.p_thresh;
-    return;
-  }
-  const double q = xyM * xyM, den = xxM * P.yyM;
-  if (P.refine && q >= P.r2_ref * den) {
-    cand = true;
-  } else if (q >= P.r2_cand * den) {
-    double r2 = q / den;
-    if (r2 < 0) r2 = 0;
-    if (r2 >= 1) r2 = 1 - 1e-15;
-    T = (double)n * log(1.0 / (1.0 - r2));
-    p = erfc(sqrt(0.5 * T));
-    effect = xyM / den;
-    hit = p <= P.p_thresh;
-  }
-}
-
-template <int NP>
+template <int NP, int PPG>
 __global__ void __launch_bounds__(MP_THREADS, 1)
     mp_kernel(const __grid_constant__ CUtensorMap tmap, unsigned long long m, int nbox, int nchunk, int G,
               int xs_slots, int nb, int S, int NA, const int8_t* __restrict__ Bimg, const MPheno* __restrict__ ph,
               const DevOutMP O) {
-  constexpr int PPG = 128 / NP;
   constexpr int N = PPG * NP;
+  static_assert(N <= 128, "phenotype group wider than one MMA");
   const int A0 = mp_a0(N, S, NA);
   const int AST = mp_ast(N, S, NA);
   constexpr uint32_t IDESC = idesc_i8(MP_TM, N);
@@ -204,10 +123,10 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
       uint32_t it = 0;
       for (unsigned long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
         const uint32_t xs = it % xs_slots, u = it / xs_slots;
-        if (u > 0 && !mp_wait(x_empty + 8 * xs, (u - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_FULL)) break;
+        if (u > 0 && !wait_or_abort(x_empty + 8 * xs, (u - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_FULL)) break;
         mbar_arrive_expect_tx(x_full + 8 * xs, xslot);
         for (int bx = 0; bx < nbox; ++bx)
-          mp_tma_2d(sx + xs * xslot + bx * MP_BOXB, &tmap, bx * 128, (int)(tile * MP_TM), x_full + 8 * xs);
+          tma_load_2d(sx + xs * xslot + bx * MP_BOXB, &tmap, bx * 128, (int)(tile * MP_TM), x_full + 8 * xs);
         last_use[xs] = u;
       }
       for (int s = 0; s < xs_slots; ++s)
@@ -224,7 +143,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
         for (int gi = 0; gi < G && ok; ++gi)
           for (int kc = 0; kc < nchunk; ++kc, ++h) {
             const uint32_t s = h % nb, u = h / nb;
-            if (u > 0 && !mp_wait(b_empty + 8 * s, (u - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_FULL)) {
+            if (u > 0 && !wait_or_abort(b_empty + 8 * s, (u - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_FULL)) {
               ok = false;
               break;
             }
@@ -243,15 +162,15 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
       for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         for (int gi = 0; gi < G && ok; ++gi, ++w) {
           const uint32_t b = w % NA, v = w / NA;
-          if (v > 0 && !mp_wait(acc_empty + 8 * b, (v - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA)) {
+          if (v > 0 && !wait_or_abort(acc_empty + 8 * b, (v - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA)) {
             ok = false;
             break;
           }
           tc_fence_after();
           for (int kc = 0; kc < nchunk; ++kc, ++g, ++h) {
             const uint32_t t = g % AST, s = h % nb;
-            if (!mp_wait(a_full + 8 * t, (g / AST) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA) ||
-                !mp_wait(b_full + 8 * s, (h / nb) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA)) {
+            if (!wait_or_abort(a_full + 8 * t, (g / AST) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA) ||
+                !wait_or_abort(b_full + 8 * s, (h / nb) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA)) {
               ok = false;
               break;
             }
@@ -281,7 +200,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
     bool ok = true;
     for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
       const uint32_t xs = it % xs_slots;
-      if (!__all_sync(0xffffffffu, mp_wait(x_full + 8 * xs, (it / xs_slots) & 1, s_abort, O.counters,
+      if (!__all_sync(0xffffffffu, wait_or_abort(x_full + 8 * xs, (it / xs_slots) & 1, s_abort, O.counters,
                                            ERR_TIMEOUT_FULL)))
         break;
       const uint32_t tb = sx + xs * xslot;
@@ -289,7 +208,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
         for (int kc = 0; kc < nchunk; ++kc, ++g) {
           if ((int)(g % MP_UG) != grp) continue;
           const uint32_t t = g % AST, u = g / AST;
-          if (u > 0 && !__all_sync(0xffffffffu, mp_wait(a_empty + 8 * t, (u - 1) & 1, s_abort, O.counters,
+          if (u > 0 && !__all_sync(0xffffffffu, wait_or_abort(a_empty + 8 * t, (u - 1) & 1, s_abort, O.counters,
                                                          ERR_TIMEOUT_MMA))) {
             ok = false;
             break;
@@ -301,11 +220,8 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
                        : "r"(tb + bx * MP_BOXB + r * 128 + ((c ^ (r & 7)) << 4)));
           const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
           uint32_t o[32];
-#pragma unroll
-          for (int qq = 0; qq < 4; ++qq)
-#pragma unroll
-            for (int j = 0; j < 8; ++j) o[qq * 8 + j] = (w4[qq] * (1u << (7 - j))) & 0x80808080u;
-          mp_st32(tmem + lane_base + A0 + t * 32, o);
+          unpack_stage(w4, o);
+          tc_st32(tmem + lane_base + A0 + t * 32, o);
           tc_wait_st();
           tc_fence_before();
           __syncwarp();
@@ -332,7 +248,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
       const bool leader = lane == __ffs(match) - 1;
       for (int gi = 0; gi < G; ++gi, ++w) {
         const uint32_t b = w % NA, v = w / NA;
-        if (!__all_sync(0xffffffffu, mp_wait(acc_full + 8 * b, v & 1, s_abort, O.counters, ERR_TIMEOUT_MMA))) {
+        if (!__all_sync(0xffffffffu, wait_or_abort(acc_full + 8 * b, v & 1, s_abort, O.counters, ERR_TIMEOUT_MMA))) {
           ok = false;
           break;
         }
@@ -360,71 +276,37 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
           const MPheno& ME = ph[p];
           const int k = ME.P.k;
           const int drop0 = ME.drop0;
+          // Limb sums hold -128 * integer sums only after recombination (half
+          // the samples enter as 64 x against the digits of -2 V): recombine
+          // exactly in int64 first, as kernel_ts.cu does.
           const int c = (-(int)d[0]) >> 7;
-          double vy = (double)((-(int)d[1]) >> 7);
+          const double cd = i2d_exact(c);
+          long long Vy = (long long)(int)d[MP_LY];
 #pragma unroll
-          for (int l = 1; l < MP_LY; ++l) vy = fma(vy, 256.0, (double)((-(int)d[1 + l]) >> 7));
-          const double ey = vy * ME.LM.scale[k];
+          for (int l = 1; l < MP_LY; ++l) Vy += (long long)(int)d[MP_LY - l] * (1ll << (8 * l));
+          const double sy = ME.LM.scale[k];
+          const double ey = fma(magic_raw((-Vy) >> 7), sy, -MAGIC_BIAS * sy);
           double ss = 0, gs = 0;
           if (drop0) {
-            const double s0 = ME.P.a[0] * (double)c;
+            const double s0 = ME.P.a[0] * cd;
             ss = s0 * s0;
           }
 #pragma unroll
           for (int jj = 0; jj < KU_MAX; ++jj) {
             const int j = jj + drop0;
-            if (j < k) {
-              const int o = 1 + MP_LY + MP_LU * jj;
-              double vj = (double)((-(int)d[o]) >> 7);
+            const int o = 1 + MP_LY + MP_LU * jj;
+            long long Vb = (long long)(int)d[o + MP_LU - 1] + (long long)0x4338000000000000LL;
 #pragma unroll
-              for (int l = 1; l < MP_LU; ++l) vj = fma(vj, 256.0, (double)((-(int)d[o + l]) >> 7));
-              const double e = vj * ME.LM.scale[j];
-              const double sj = fma(ME.P.a[j], (double)c, e);
-              ss = fma(sj, sj, ss);
-              gs = fma(ME.P.g[j], e, gs);
-            }
+            for (int l = 1; l < MP_LU; ++l) Vb += (long long)(int)d[o + MP_LU - 1 - l] * (1ll << (8 * l));
+            const double e = fma(__longlong_as_double(Vb), ME.LM.esc[j], ME.LM.eoff[j]);
+            const double sj = fma(ME.P.a[j], cd, e);
+            ss = fma(sj, sj, ss);
+            gs = fma(ME.P.g[j], e, gs);
           }
           bool tested, hit, cand;
           double T, pv, effect;
           mp_eval(ME.P, valid, c, ss, gs, ey, tested, hit, cand, T, pv, effect);
-          // tested count of (shard, phenotype): one atomic per shard present in the warp
-          const unsigned tm = __ballot_sync(0xffffffffu, tested);
-          if (leader && (tm & match))
-            atomicAdd(O.tested + (size_t)shard * O.n_pheno + p, (unsigned long long)__popc(tm & match));
-          const unsigned hm = __ballot_sync(0xffffffffu, hit);
-          if (hm) {
-            unsigned long long hb = 0;
-            const int hl = __ffs(hm) - 1;
-            if (lane == hl) hb = atomicAdd(O.counters + 1, (unsigned long long)__popc(hm));
-            hb = __shfl_sync(0xffffffffu, hb, hl);
-            if (hit) {
-              const unsigned long long slot = hb + __popc(hm & ((1u << lane) - 1u));
-              if (slot < O.hit_cap) {
-                kg_phit hrec;
-                hrec.kmer = gk;
-                hrec.pheno = p;
-                hrec.shard = shard;
-                hrec.effect = effect;
-                hrec.pval = pv;
-                hrec.chisq = T;
-                O.hits[slot] = hrec;
-              } else {
-                atomicOr(O.counters + 2, (unsigned long long)ERR_HIT_OVERFLOW);
-              }
-            }
-          }
-          const unsigned cm = __ballot_sync(0xffffffffu, cand);
-          if (cm) {
-            unsigned long long cb = 0;
-            const int cl = __ffs(cm) - 1;
-            if (lane == cl) cb = atomicAdd(O.counters + 3, (unsigned long long)__popc(cm));
-            cb = __shfl_sync(0xffffffffu, cb, cl);
-            if (cand) {
-              const unsigned long long slot = cb + __popc(cm & ((1u << lane) - 1u));
-              if (slot < O.cand_cap) O.cand[slot] = gk | ((unsigned long long)p << 48);
-              else atomicOr(O.counters + 2, (unsigned long long)ERR_CAND_OVERFLOW);
-            }
-          }
+          mp_emit(O, p, gk, shard, match, leader, tested, hit, cand, T, pv, effect);
         }
         tc_fence_before();
         __syncwarp();
@@ -507,18 +389,18 @@ static PFN_cuTensorMapEncodeTiled_v12000 mp_encode_fn() {
 
 size_t mp_smem_bytes(int nbox, int xs, int nb, int N) { return mp_smem(nbox, xs, nb, N).total + 1024; }
 
-bool mp_supported(int NP, int wpk) {
-  if (NP < 16 || NP > 128 || NP % 16) return false;
+bool mp_supported(int NP, int PPG, int wpk) {
+  if (NP < 16 || NP > 128 || NP % 16 || PPG < 1 || NP * PPG > 128) return false;
   if (wpk * 8 < 128) return false;
   return mp_encode_fn() != nullptr;
 }
 
-template <int NP>
+template <int NP, int PPG>
 static cudaError_t launch_mp_t(const LaunchMp& L, const CUtensorMap& tm, cudaStream_t st) {
-  constexpr int N = (128 / NP) * NP;
+  constexpr int N = PPG * NP;
   const int nbox = (L.wpk * 8 + 127) / 128;
   const size_t smem = mp_smem_bytes(nbox, L.xs, L.nb, N);
-  cudaError_t e = cudaFuncSetAttribute(mp_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(mp_kernel<NP, PPG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const unsigned long long tiles = (L.m + MP_TM - 1) / MP_TM;
   unsigned long long grid = (unsigned long long)L.num_sms;
@@ -528,35 +410,32 @@ static cudaError_t launch_mp_t(const LaunchMp& L, const CUtensorMap& tm, cudaStr
     S = 1;
     NA = 2;
   }
-  mp_kernel<NP><<<(unsigned)grid, MP_THREADS, smem, st>>>(tm, L.m, nbox, L.kpad / MP_KS, L.G, L.xs, L.nb, S, NA,
-                                                          L.Bimg, L.ph, *L.O);
+  mp_kernel<NP, PPG><<<(unsigned)grid, MP_THREADS, smem, st>>>(tm, L.m, nbox, L.kpad / MP_KS, L.G, L.xs, L.nb, S,
+                                                               NA, L.Bimg, L.ph, *L.O);
   return cudaGetLastError();
 }
 
-cudaError_t launch_mp(const LaunchMp& L, cudaStream_t st) {
+bool mp_tmap(const uint64_t* x, unsigned long long m, int wpk, CUtensorMap* tm) {
   auto enc = mp_encode_fn();
-  if (!enc) return cudaErrorNotSupported;
-  CUtensorMap tm;
-  const cuuint64_t rowbytes = (cuuint64_t)L.wpk * 8;
-  cuuint64_t gdim[2] = {rowbytes, (cuuint64_t)L.m};
+  if (!enc) return false;
+  const cuuint64_t rowbytes = (cuuint64_t)wpk * 8;
+  cuuint64_t gdim[2] = {rowbytes, (cuuint64_t)m};
   cuuint64_t gstride[1] = {rowbytes};
   cuuint32_t box[2] = {128, MP_TM};
   cuuint32_t estr[2] = {1, 1};
-  if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)L.x, gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-    return cudaErrorInvalidValue;
-  switch (L.NP) {
-    case 16: return launch_mp_t<16>(L, tm, st);
-    case 32: return launch_mp_t<32>(L, tm, st);
-    case 48: return launch_mp_t<48>(L, tm, st);
-    case 64: return launch_mp_t<64>(L, tm, st);
-    case 80: return launch_mp_t<80>(L, tm, st);
-    case 96: return launch_mp_t<96>(L, tm, st);
-    case 112: return launch_mp_t<112>(L, tm, st);
-    case 128: return launch_mp_t<128>(L, tm, st);
-    default: return cudaErrorInvalidValue;
-  }
+  return enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)x, gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+cudaError_t launch_mp(const LaunchMp& L, cudaStream_t st) {
+  CUtensorMap tm;
+  if (!mp_tmap(L.x, L.m, L.wpk, &tm)) return cudaErrorInvalidValue;
+#define KG_MP_CASE(NP_, PPG_) \
+  if (L.NP == NP_ && L.PPG == PPG_) return launch_mp_t<NP_, PPG_>(L, tm, st);
+  KG_MP_GROUPS(KG_MP_CASE)
+#undef KG_MP_CASE
+  return cudaErrorInvalidValue;
 }
 
 template <int CM>

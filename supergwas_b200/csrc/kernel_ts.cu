@@ -76,72 +76,6 @@ __host__ __device__ inline TsSmem ts_smem(int b_bytes) {
   return L;
 }
 
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const void* tmap, int x, int y, uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          dst),
-      "l"(tmap), "r"(x), "r"(y), "r"(bar)
-      : "memory");
-}
-
-__device__ __forceinline__ void tc_st32(uint32_t taddr, const uint32_t (&r)[32]) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
-      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
-      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
-      "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]),
-      "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]),
-      "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
-      : "memory");
-}
-
-// 128 packed samples (four 32-bit words) -> 32 TMEM columns of int8 A
-// operand: column 8q+jj holds, in byte t, sample 32q + 8t + 7 - jj as -128 x
-// (jj even) or 64 x (jj odd).  make_b_image_ts lays B out to match.
-__device__ __forceinline__ void unpack_stage(const uint32_t (&w)[4], uint32_t (&o)[32]) {
-#pragma unroll
-  for (int qq = 0; qq < 4; ++qq)
-#pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      const uint32_t u = w[qq] * (1u << (2 * h));
-      o[qq * 8 + 2 * h] = u & 0x80808080u;
-      o[qq * 8 + 2 * h + 1] = u & 0x40404040u;
-    }
-}
-
-// Bounded wait that also gives up when another role has aborted.  The first
-// test is inline (the common case: the phase is already complete); the
-// abort flag and the clock are read only every 16 failed tests.
-__device__ __forceinline__ bool ts_wait(uint32_t bar, uint32_t parity, volatile int* abort,
-                                        unsigned long long* counters, unsigned code) {
-  if (mbar_try(bar, parity)) return true;
-  const unsigned long long t0 = gtimer_ns();
-  for (uint32_t it = 1;; ++it) {
-    if (mbar_try(bar, parity)) return true;
-    if ((it & 15u) == 0) {
-      if (*abort) return false;
-      if (gtimer_ns() - t0 > WAIT_LIMIT_NS) {
-        atomicOr(counters + 2, (unsigned long long)code);
-        *abort = 1;
-        return false;
-      }
-    }
-  }
-}
-
-// Ring position: slot index and phase parity, advanced without division.
-template <int NS>
-struct Ring {
-  uint32_t slot = 0, phase = 0, used = 0;  // used: laps completed (0 = first)
-  __device__ __forceinline__ void next() {
-    if (++slot == (uint32_t)NS) {
-      slot = 0;
-      phase ^= 1u;
-      used = 1;
-    }
-  }
-};
-
 template <int N, bool DROP0>
 __global__ void __launch_bounds__(ts_threads(N), 1)
     ts_kernel(const __grid_constant__ CUtensorMap tmap, unsigned long long m, int nbox, int nsub,
@@ -215,7 +149,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
       bool ok = true;
       for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         for (int bx = 0; bx < nbox; ++bx, xr.next()) {
-          if (xr.used && !ts_wait(x_empty + 8 * xr.slot, xr.phase ^ 1u, s_abort, O.counters, ERR_TIMEOUT_FULL)) {
+          if (xr.used && !wait_or_abort(x_empty + 8 * xr.slot, xr.phase ^ 1u, s_abort, O.counters, ERR_TIMEOUT_FULL)) {
             ok = false;
             break;
           }
@@ -235,13 +169,13 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
     // The whole warp runs the loop (warp-uniform control flow and operands);
     // one elected lane issues the MMAs and the commits that track them.
     const bool leader = elect_one();
-    bool ok = __all_sync(0xffffffffu, ts_wait(b_full, 0, s_abort, O.counters, ERR_TIMEOUT_FULL));
+    bool ok = __all_sync(0xffffffffu, wait_or_abort(b_full, 0, s_abort, O.counters, ERR_TIMEOUT_FULL));
     const uint64_t bdesc0 = sdesc_noswz(sb, N * 16, 128);
     Ring<NSLOT> ar;
     uint32_t i = 0;
     for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++i) {
       const uint32_t b = i & 1u;
-      if (i >= 2 && !__all_sync(0xffffffffu, ts_wait(acc_empty + 8 * b, ((i >> 1) - 1) & 1u, s_abort, O.counters,
+      if (i >= 2 && !__all_sync(0xffffffffu, wait_or_abort(acc_empty + 8 * b, ((i >> 1) - 1) & 1u, s_abort, O.counters,
                                                      ERR_TIMEOUT_MMA))) {
         ok = false;
         break;
@@ -249,7 +183,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
       const uint32_t d_t = tmem + b * N;
       uint64_t bd = bdesc0;
       for (int sp = 0; sp < nsp; ++sp, ar.next()) {
-        if (!__all_sync(0xffffffffu, ts_wait(a_full + 8 * ar.slot, ar.phase, s_abort, O.counters, ERR_TIMEOUT_MMA))) {
+        if (!__all_sync(0xffffffffu, wait_or_abort(a_full + 8 * ar.slot, ar.phase, s_abort, O.counters, ERR_TIMEOUT_MMA))) {
           ok = false;
           break;
         }
@@ -302,7 +236,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
       for (int bx = 0; bx < nbox && ok; ++bx, xr.next()) {
         // every unpack warp waits for every box, also one holding none of its
         // super-stages, so that its release below belongs to this fill
-        if (!__all_sync(0xffffffffu, ts_wait(x_full + 8 * xr.slot, xr.phase, s_abort, O.counters,
+        if (!__all_sync(0xffffffffu, wait_or_abort(x_full + 8 * xr.slot, xr.phase, s_abort, O.counters,
                                             ERR_TIMEOUT_FULL))) {
           ok = false;
           break;
@@ -317,7 +251,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
             turn ^= 1u;
             continue;
           }
-          if (ar.used && !__all_sync(0xffffffffu, ts_wait(a_empty + 8 * ar.slot, ar.phase ^ 1u, s_abort,
+          if (ar.used && !__all_sync(0xffffffffu, wait_or_abort(a_empty + 8 * ar.slot, ar.phase ^ 1u, s_abort,
                                                           O.counters, ERR_TIMEOUT_MMA))) {
             ok = false;
             break;
@@ -381,7 +315,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
     uint32_t tested_local = 0;  // k-mers this thread tested (lean path)
     for (unsigned long long tile = blockIdx.x + (unsigned long long)e * gridDim.x; tile < ntiles;
          tile += 2ull * gridDim.x, ++jt) {
-      if (!__all_sync(0xffffffffu, ts_wait(acc_full + 8 * e, jt & 1u, s_abort, O.counters, ERR_TIMEOUT_MMA))) break;
+      if (!__all_sync(0xffffffffu, wait_or_abort(acc_full + 8 * e, jt & 1u, s_abort, O.counters, ERR_TIMEOUT_MMA))) break;
       tc_fence_after();
       uint32_t d[N];
 #pragma unroll

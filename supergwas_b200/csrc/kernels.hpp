@@ -4,6 +4,8 @@
 
 #include "params.hpp"
 
+struct CUtensorMap_st;
+
 namespace kg {
 
 struct LaunchFp64 {
@@ -67,13 +69,20 @@ struct LaunchTs {
 bool ts_supported(int N, int limbs_u, int limbs_y, int kpad, int wpk);
 cudaError_t launch_ts(const LaunchTs& L, cudaStream_t st);
 
+// (columns per phenotype slot, phenotypes per group) pairs with a compiled
+// many-phenotype kernel; the group width NP * PPG is at most 128.
+#define KG_MP_GROUPS(X)                                                                      \
+  X(16, 1) X(16, 2) X(16, 4) X(16, 8) X(32, 1) X(32, 2) X(32, 4) X(48, 1) X(48, 2) X(64, 1) \
+  X(64, 2) X(80, 1) X(96, 1) X(112, 1) X(128, 1)
+
 struct LaunchMp {
   const uint64_t* x;          // packed rows (device), 16-byte aligned
   unsigned long long m;
   int wpk;
   int kpad;                   // samples per phenotype group image (multiple of 128)
   int NP;                     // columns per phenotype slot (multiple of 16, <= 128)
-  int G;                      // phenotype groups (128 / NP phenotypes each)
+  int PPG;                    // phenotypes per group (KG_MP_GROUPS)
+  int G;                      // phenotype groups
   int xs, nb;                 // resident x tiles (1-2), B ring stages (2-8)
   int splits, nacc;           // split-K accumulators, accumulator buffers (0: default)
   const int8_t* Bimg;         // G x (kpad/128) chunks of 128 x N bytes (device)
@@ -92,9 +101,30 @@ struct LaunchMpRefine {
   int num_sms;
   const double* T = nullptr;  // byte tables of V, refine_table_len(vrows, cm) doubles per phenotype
 };
-bool mp_supported(int NP, int wpk);
+bool mp_supported(int NP, int PPG, int wpk);
 size_t mp_smem_bytes(int nbox, int xs, int nb, int N);
 cudaError_t launch_mp(const LaunchMp& L, cudaStream_t st);
+// 2-D TMA map of packed rows: 128-byte x 128-row boxes, 128-byte swizzle.
+bool mp_tmap(const uint64_t* x, unsigned long long m, int wpk, CUtensorMap_st* tm);
+
+// B-stationary many-phenotype kernel (kernel_mpb.cu): each group's image
+// (make_b_image_ts layout, kpad x NP*PPG bytes) resident in shared memory for
+// a pass over `bt` tile-iterations of every CTA.
+struct LaunchMpb {
+  const uint64_t* x;
+  unsigned long long m;
+  int wpk;
+  int kpad;
+  int NP, PPG, G;
+  int bt;                     // tile-iterations per L2 block
+  const int8_t* Bimg;         // G images of kpad x NP*PPG bytes (device)
+  const MPheno* ph;
+  const DevOutMP* O;
+  int num_sms;
+};
+bool mpb_supported(int NP, int PPG, int kpad, int wpk);  // the image and the x ring fit in shared memory
+size_t mpb_smem_bytes(int N, int kpad);
+cudaError_t launch_mpb(const LaunchMpb& L, cudaStream_t st);
 cudaError_t launch_mp_refine(const LaunchMpRefine& L, cudaStream_t st);
 
 int tc_kc();                  // samples per K chunk of the tensor-core kernel

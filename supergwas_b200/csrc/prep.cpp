@@ -179,11 +179,10 @@ std::string make_limbs(const Prepared& p, const int* pos, int n_row, int limbs_u
   return "";
 }
 
-void make_b_image_ts(const LimbCols& L, std::vector<int8_t>& img) {
-  const int N = L.N;
+void put_b_image_ts(const LimbCols& L, int col0, int N, std::vector<int8_t>& img) {
   // Limb digits of -2 V for every sample, column by column (V = the value a
   // logical column's digits encode; the count column holds V = 1).
-  std::vector<int8_t> neg2((size_t)N * L.Kpad, 0);
+  std::vector<int8_t> neg2((size_t)L.N * L.Kpad, 0);
   std::vector<int8_t> dg(8);
   auto regroup = [&](int first, int nl) {
     for (int i = 0; i < L.Kpad; ++i) {
@@ -195,22 +194,27 @@ void make_b_image_ts(const LimbCols& L, std::vector<int8_t>& img) {
   };
   regroup(L.count_col, 1);
   for (int j = 0; j <= KMAX; ++j)
-    if (L.nl[j] > 0 && L.first[j] > 0 && L.first[j] + L.nl[j] <= N) regroup(L.first[j], L.nl[j]);
-  img.assign((size_t)L.Kpad * N, 0);
+    if (L.nl[j] > 0 && L.first[j] > 0 && L.first[j] + L.nl[j] <= L.N) regroup(L.first[j], L.nl[j]);
   for (int kap = 0; kap < L.Kpad; ++kap) {
-    // TMEM column c of a 128-sample stage holds K = 4c..4c+3.  The unpack in
-    // kernel_ts.cu writes, for 32-bit word q of the stage and jj = 0..7,
-    // column 8q+jj = (word << 2*(jj/2)) & (jj even ? 0x80808080 : 0x40404040):
-    // byte t of it is sample 32q + 8t + 7 - jj, as -128 x (jj even) or 64 x
-    // (jj odd).  Odd columns therefore take the digits of -2 V.
+    // TMEM column c of a 128-sample stage holds K = 4c..4c+3.  The unpack
+    // (unpack_stage in device.cuh) writes, for 32-bit word q of the stage and
+    // jj = 0..7, column 8q+jj = (word << 2*(jj/2)) & (jj even ? 0x80808080 :
+    // 0x40404040): byte t of it is sample 32q + 8t + 7 - jj, as -128 x (jj
+    // even) or 64 x (jj odd).  Odd columns therefore take the digits of -2 V.
     const int a = kap / 128, w = kap % 128, c = w / 4, t = w % 4, q = c / 8, jj = c % 8;
     const int i = 128 * a + 32 * q + 8 * t + 7 - jj;
     const std::vector<int8_t>& src = (jj & 1) ? neg2 : L.vals;
-    for (int col = 0; col < N; ++col) {
-      const size_t off = (size_t)(kap / 16) * (N * 16) + (size_t)(col / 8) * 128 + (size_t)(col % 8) * 16 + kap % 16;
+    for (int col = 0; col < L.N; ++col) {
+      const int cc = col0 + col;
+      const size_t off = (size_t)(kap / 16) * (N * 16) + (size_t)(cc / 8) * 128 + (size_t)(cc % 8) * 16 + kap % 16;
       img[off] = src[(size_t)col * L.Kpad + i];
     }
   }
+}
+
+void make_b_image_ts(const LimbCols& L, std::vector<int8_t>& img) {
+  img.assign((size_t)L.Kpad * L.N, 0);
+  put_b_image_ts(L, 0, L.N, img);
 }
 
 void make_b_image(const LimbCols& L, int KC, std::vector<int8_t>& img) {

@@ -68,10 +68,15 @@ std::string make_limbs(const Prepared& p, const int* pos, int n_row, int limbs_u
 // (n8, k16) of chunk q at q*KC*N + k16*(N*16) + n8*128).
 void make_b_image(const LimbCols& L, int KC, std::vector<int8_t>& img);
 
-// B operand image for the TMEM-A kernel: the whole Kpad x N matrix in one
+// B operand image for the TMEM-A kernels: the whole Kpad x N matrix in one
 // K-major no-swizzle layout (core (n8, k16) at k16*(N*16) + n8*128), with the
 // K index permuted inside every 128-sample stage to match the bit unpack
-// order: K = 4c + t of column c = 8q + j holds sample 32q + 8t + j.
+// order: K = 4c + t of column c = 8q + j holds sample 32q + 8t + 7 - j, with
+// the digits of V for even j and of -2 V for odd j.
 void make_b_image_ts(const LimbCols& L, std::vector<int8_t>& img);
+// The columns of L at columns col0 .. col0 + L.N - 1 of an N-column image in
+// the same layout (img holds L.Kpad * N bytes): several phenotypes side by
+// side in one MMA.
+void put_b_image_ts(const LimbCols& L, int col0, int N, std::vector<int8_t>& img);
 
 }  // namespace kg

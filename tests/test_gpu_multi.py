@@ -41,9 +41,14 @@ def oracle_pheno(packed_all, n_all, U, y, keep, thr):
     return O.cols_stats(synth.select_samples(packed_all, n_all, keep), keep.size, U, y, thr)
 
 
+@pytest.mark.parametrize("kernel", ["stationary", "streamed"])
 @pytest.mark.parametrize("case", [(1000, 6000, 5, (16,), 16), (2000, 3000, 9, (20, 4), 32),
                                   (300, 2500, 7, (3, 6), 16)], ids=["n1000_r16", "n2000_r20", "n300_r3"])
-def test_multi_matches_oracle(built, case):
+def test_multi_matches_oracle(built, case, kernel, monkeypatch):
+    """Both many-phenotype kernels: the B image resident in shared memory
+    (kernel_mpb.cu) and streamed from L2 per 128 samples (kernel_mp.cu)."""
+    if kernel == "streamed":
+        monkeypatch.setenv("KG_MP_STREAMED", "1")
     n_all, m, npheno, rl, wpk = case
     packed, phenos = make_batch(n_all, m, npheno, rl, seed=n_all + m, wpk=wpk)
     shards = np.array([0, 7, m // 3, m // 3 + 1, m - 5], dtype=np.uint64)
@@ -111,3 +116,28 @@ def test_multi_streamed_chunks_match_single_chunk(built, monkeypatch):
         t2, h2 = g.run_multi_host(packed, shards)
     assert np.array_equal(t1, t2)
     assert np.array_equal(h1, h2)
+
+
+def test_multi_kernels_bit_identical(built, monkeypatch):
+    """The B-stationary and streamed-B kernels give the same counts and the
+    same rows bit for bit (same limb image, same exact integer sums), also
+    with several L2 blocks per launch and a partial last block."""
+    n_all, m = 2000, 50000
+    packed, phenos = make_batch(n_all, m, 6, (20, 9), seed=23, wpk=32)
+    shards = np.array([0, 4096, 30001], dtype=np.uint64)
+    out = {}
+    for kernel, bt in (("stationary", None), ("stationary", "2"), ("streamed", None)):
+        monkeypatch.delenv("KG_MP_STREAMED", raising=False)
+        monkeypatch.delenv("KG_MP_BT", raising=False)
+        if kernel == "streamed":
+            monkeypatch.setenv("KG_MP_STREAMED", "1")
+        if bt:
+            monkeypatch.setenv("KG_MP_BT", bt)
+        with api.Kgwas(corr_threshold=0.0, log10_thresh=1.0) as g:
+            g.set_phenotypes(phenos, n_all)
+            out[(kernel, bt)] = g.run_multi_host(packed, shards)
+    t0, h0 = out[("streamed", None)]
+    for key in (("stationary", None), ("stationary", "2")):
+        t, h = out[key]
+        assert np.array_equal(t, t0), key
+        assert np.array_equal(h, h0), key
