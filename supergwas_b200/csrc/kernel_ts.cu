@@ -47,7 +47,10 @@ constexpr int TS_TM = 128;
 constexpr int TS_KS = 128;         // samples per sub-stage (32 TMEM columns, 4 MMAs)
 constexpr int TS_SUPER = 4;        // sub-stages per super-stage (one barrier, one commit)
 constexpr int TS_BOX = 1024;       // samples per TMA box (128 bytes)
-constexpr int TS_XST = 4;          // packed boxes in flight
+// Packed boxes in flight: as many as the shared memory left by the B image
+// holds, up to TS_XST_MAX (chosen at launch).  HBM latency under this load is
+// ~2 us, so 4 boxes (64 KB per SM) cap the row stream near 4.3 TB/s.
+constexpr int TS_XST_MAX = 12;
 // Unpack groups (taking super-stages in turn): two while the epilogue fits
 // the register budget of 18 warps, one for wide N.
 __host__ __device__ constexpr int ts_ug(int N) { return N <= 80 ? 2 : 1; }
@@ -65,12 +68,12 @@ __host__ __device__ constexpr int ts_nslot(int N) {
 struct TsSmem {  // offsets from the 1024-aligned base
   uint32_t x, b, bars, tmem, abort, total;
 };
-__host__ __device__ inline TsSmem ts_smem(int b_bytes) {
+__host__ __device__ inline TsSmem ts_smem(int b_bytes, int xst) {
   TsSmem L;
   L.x = 0;
-  L.b = TS_XST * TS_XBYTES;
+  L.b = xst * TS_XBYTES;
   L.bars = L.b + ((b_bytes + 127) / 128) * 128;
-  L.tmem = L.bars + 8 * (2 * TS_XST + 2 * TS_MAXSLOT + 4 + 2);
+  L.tmem = L.bars + 8 * (2 * TS_XST_MAX + 2 * TS_MAXSLOT + 4 + 2);
   L.abort = L.tmem + 8;
   L.total = L.abort + 8;
   return L;
@@ -78,7 +81,7 @@ __host__ __device__ inline TsSmem ts_smem(int b_bytes) {
 
 template <int N, bool DROP0>
 __global__ void __launch_bounds__(ts_threads(N), 1)
-    ts_kernel(const __grid_constant__ CUtensorMap tmap, unsigned long long m, int nbox, int nsub,
+    ts_kernel(const __grid_constant__ CUtensorMap tmap, unsigned long long m, int nbox, int nsub, int xst,
               const int8_t* __restrict__ Bimg, int b_bytes, const __grid_constant__ EpiParams P,
               const __grid_constant__ LimbMap LM, const DevOut O) {
   constexpr int UG = ts_ug(N);
@@ -93,10 +96,10 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   uint8_t* gbase = smem_raw + (base - raw);
-  const TsSmem L = ts_smem(b_bytes);
+  const TsSmem L = ts_smem(b_bytes, xst);
   const uint32_t sx = base + L.x, sb = base + L.b;
-  const uint32_t x_full = base + L.bars, x_empty = x_full + 8 * TS_XST;
-  const uint32_t a_full = x_empty + 8 * TS_XST, a_empty = a_full + 8 * TS_MAXSLOT;
+  const uint32_t x_full = base + L.bars, x_empty = x_full + 8 * TS_XST_MAX;
+  const uint32_t a_full = x_empty + 8 * TS_XST_MAX, a_empty = a_full + 8 * TS_MAXSLOT;
   const uint32_t acc_full = a_empty + 8 * TS_MAXSLOT, acc_empty = acc_full + 16, b_full = acc_empty + 16;
   const uint32_t drain = b_full + 8;
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(gbase + L.tmem);
@@ -110,7 +113,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 32) {
-    for (int s = 0; s < TS_XST; ++s) {
+    for (int s = 0; s < xst; ++s) {
       mbar_init(x_full + 8 * s, 1);
       mbar_init(x_empty + 8 * s, 4 * UG);  // every unpack warp
     }
@@ -142,10 +145,10 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
         const int len = b_bytes - off < 32768 ? b_bytes - off : 32768;
         bulk_g2s(sb + off, Bimg + off, (uint32_t)len, b_full);
       }
-      Ring<TS_XST> xr;
-      uint32_t last_phase[TS_XST];
-      bool issued[TS_XST];
-      for (int s = 0; s < TS_XST; ++s) issued[s] = false, last_phase[s] = 0;
+      RingN xr(xst);
+      uint32_t last_phase[TS_XST_MAX];
+      bool issued[TS_XST_MAX];
+      for (int s = 0; s < TS_XST_MAX; ++s) issued[s] = false, last_phase[s] = 0;
       bool ok = true;
       for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         for (int bx = 0; bx < nbox; ++bx, xr.next()) {
@@ -161,7 +164,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
       }
       // no copy may still be landing when the block exits
       mbar_wait(b_full, 0, O.counters, ERR_TIMEOUT_FULL);
-      for (int s = 0; s < TS_XST; ++s)
+      for (int s = 0; s < xst; ++s)
         if (issued[s]) mbar_wait(x_full + 8 * s, last_phase[s], O.counters, ERR_TIMEOUT_FULL);
     }
   } else if (warp == TS_WARP_MMA) {
@@ -227,7 +230,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
     const int q = warp & 3;                         // TMEM lane quarter
     const int r = q * 32 + lane;                    // row of the tile = TMEM lane
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
-    Ring<TS_XST> xr;
+    RingN xr(xst);
     Ring<NSLOT> ar;
     uint32_t turn = 0;  // super-stage counter parity
     bool ok = true;
@@ -402,10 +405,25 @@ bool ts_supported(int N, int limbs_u, int limbs_y, int kpad, int wpk) {
   return encode_fn() != nullptr;
 }
 
+// Boxes of the packed-row ring that fit next to the B image (at least 2).
+static int ts_ring_depth(int b_bytes) {
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) optin = 0;
+  int x = TS_XST_MAX;
+  while (x > 2 && ts_smem(b_bytes, x).total + 1024 > (uint32_t)optin) --x;
+  if (const char* v = std::getenv("KG_TS_XST")) {
+    const int want = std::atoi(v);
+    if (want >= 2 && want < x) x = want;
+  }
+  return x;
+}
+
 template <int N, bool D0>
 static cudaError_t launch_ts_t(const LaunchTs& L, const CUtensorMap& tm, cudaStream_t st) {
   const int b_bytes = L.kpad * N;
-  const size_t smem = ts_smem(b_bytes).total + 1024;
+  const int xst = ts_ring_depth(b_bytes);
+  const size_t smem = ts_smem(b_bytes, xst).total + 1024;
   cudaError_t e = cudaFuncSetAttribute(ts_kernel<N, D0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const unsigned long long tiles = (L.m + TS_TM - 1) / TS_TM;
@@ -413,8 +431,8 @@ static cudaError_t launch_ts_t(const LaunchTs& L, const CUtensorMap& tm, cudaStr
   if (grid > tiles) grid = tiles;
   const int nbox = (L.wpk * 8 + 127) / 128;
   const int nsub = L.kpad / TS_KS;
-  ts_kernel<N, D0><<<(unsigned)grid, ts_threads(N), smem, st>>>(tm, L.m, nbox, nsub, L.Bimg, b_bytes, *L.P, *L.LM,
-                                                             *L.O);
+  ts_kernel<N, D0><<<(unsigned)grid, ts_threads(N), smem, st>>>(tm, L.m, nbox, nsub, xst, L.Bimg, b_bytes, *L.P,
+                                                             *L.LM, *L.O);
   return cudaGetLastError();
 }
 
