@@ -57,6 +57,20 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// As mbar_try, letting the hardware suspend the thread until the phase
+// completes (or about 1 ms passes) instead of returning at once, so that a
+// waiting warp takes no issue slots from the warps doing the work.
+__device__ __forceinline__ bool mbar_try_sleep(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(1000000u)
+      : "memory");
+  return ok != 0;
+}
 // Bounded wait: false (and an error bit in counters[2]) after WAIT_LIMIT_NS.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
                                           unsigned long long* counters, unsigned code) {
@@ -200,7 +214,7 @@ __device__ __forceinline__ bool wait_or_abort(uint32_t bar, uint32_t parity, vol
   if (mbar_try(bar, parity)) return true;
   const unsigned long long t0 = gtimer_ns();
   for (uint32_t it = 1;; ++it) {
-    if (mbar_try(bar, parity)) return true;
+    if (mbar_try_sleep(bar, parity)) return true;
     if ((it & 15u) == 0) {
       if (*abort) return false;
       if (gtimer_ns() - t0 > WAIT_LIMIT_NS) {
@@ -218,6 +232,18 @@ struct Ring {
   uint32_t slot = 0, phase = 0, used = 0;  // used: laps completed (0 = first)
   __device__ __forceinline__ void next() {
     if (++slot == (uint32_t)NS) {
+      slot = 0;
+      phase ^= 1u;
+      used = 1;
+    }
+  }
+};
+// The same with a size chosen at launch.
+struct RingN {
+  uint32_t slot = 0, phase = 0, used = 0, size;
+  __device__ __forceinline__ explicit RingN(uint32_t n) : size(n) {}
+  __device__ __forceinline__ void next() {
+    if (++slot == size) {
       slot = 0;
       phase ^= 1u;
       used = 1;
@@ -424,16 +450,20 @@ __device__ __forceinline__ void flush_tested(const DevOut& O, uint32_t tested_lo
 // is the sum of column j over the samples of 8-sample group g whose bit is set
 // in b.  Lane l accumulates columns l, l+32, ... over the row's bytes in
 // order, one coalesced table row per byte (instead of one V row per set bit).
-// nwords: words of the row covered by the tables.  Called by a whole warp.
+// nwords: words of the row covered by the tables.  With row2, the column is
+// the product of two rows (AND of their words: the 2-D pair test).  Called by
+// a whole warp.
 template <int CM>
 __device__ __forceinline__ void table_row_sums(const uint64_t* __restrict__ row, int nwords,
                                                const double* __restrict__ T, int lane,
-                                               double (&acc)[(CM + 31) / 32]) {
+                                               double (&acc)[(CM + 31) / 32],
+                                               const uint64_t* __restrict__ row2 = nullptr) {
   constexpr int JW = (CM + 31) / 32;
 #pragma unroll
   for (int jj = 0; jj < JW; ++jj) acc[jj] = 0.0;
   for (int w = 0; w < nwords; ++w) {
-    const uint64_t bits = __ldg(row + w);  // one address for the whole warp
+    uint64_t bits = __ldg(row + w);  // one address for the whole warp
+    if (row2) bits &= __ldg(row2 + w);
     const double* Tw = T + (size_t)w * (8 * 256 * CM);
     double v[8][JW];
 #pragma unroll
