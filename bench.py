@@ -528,6 +528,101 @@ def run_streaming(args):
     api.lib().kg_host_free(hbuf)
 
 
+PAIRS = dict(n=1000, N=50_000, S=8, r=16, seed=48, cpu_N=3000)
+
+
+def reference_pairs_run(X, n, U, y, N_cpu, threads, workdir):
+    """The reference kgwas_2d on the first N_cpu k-mers: index built by the
+    reference's build_index from a .2d.tsv of bitstrings; returns (pairs scored
+    by the oracle's rules, seconds of the kgwas_2d process)."""
+    from supergwas_b200 import synth
+    from oracle import oracle as O
+    rng = np.random.default_rng(7)
+    kmers = synth.random_kmers(rng, N_cpu, 31)
+    x = synth.unpack_rows(X[:N_cpu], n)
+    tsv = os.path.join(workdir, "hits.2d.tsv")
+    with open(tsv, "w") as f:
+        for j in range(N_cpu):
+            f.write(kmers[j] + "\t" + "".join("1" if v else "0" for v in x[j]) + "\t0\t1\n")
+    idx = os.path.join(workdir, "index")
+    r = O.run_reference_tool("build_index", [tsv, idx, "--shards", "4"])
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr[-500:])
+    ids = [f"s{i}" for i in range(n)]
+    synth.write_samples(os.path.join(workdir, "samples.txt"), ids)
+    synth.write_pheno(os.path.join(workdir, "pheno.txt"), ids, y)
+    synth.write_ubin(os.path.join(workdir, "U.bin"), U)
+    t0 = time.perf_counter()
+    r = O.run_reference_tool("kgwas_2d", [os.path.join(workdir, "samples.txt"), os.path.join(workdir, "pheno.txt"),
+                                          os.path.join(workdir, "U.bin"), idx, os.path.join(workdir, "out"), "6"],
+                             {"BLAS_THREADS": threads, "EMIT_THREADS": threads})
+    dt = time.perf_counter() - t0
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr[-500:])
+    return N_cpu * (N_cpu - 1) // 2, dt
+
+
+def run_pairs(args):
+    """2-D pair test (kgwas_2d): every pair of N k-mers, n=1000, r=16+1,
+    through kg_pairs_run_host (rows from host memory, pairs back sorted)."""
+    import torch
+    from supergwas_b200 import api, build, synth_gpu
+    rank, world, local = rank_env()
+    torch.cuda.set_device(local)
+    build.build_all()
+    W = dict(PAIRS)
+    if args.kmers:
+        W["N"] = args.kmers
+    n, N, r = W["n"], W["N"], W["r"]
+    Xd = synth_gpu.gen_packed(n, N, W["S"], W["seed"] + 1000 * rank)
+    U, _, keep, _ = synth_gpu.structure_and_phenotype(Xd, n, r, 0, 0.0, W["seed"])
+    X = Xd.cpu().numpy().view(np.uint64)
+    from supergwas_b200 import synth
+    x = synth.unpack_rows(X[:64], n).astype(np.float64)
+    rng = np.random.default_rng(W["seed"])
+    y = 1.5 * x[3] * x[17] - 1.0 * x[5] * x[9] + rng.standard_normal(n)
+    g = api.Kgwas(device=local, log10_thresh=6.0)
+    g.set_structure(U, y)
+    for _ in range(args.warmup):
+        res, n_eval = g.run_pairs_host(X)
+    torch.cuda.synchronize()
+    times = []
+    with Clocks(local) as ck:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            res, n_eval = g.run_pairs_host(X)
+            times.append(time.perf_counter() - t0)
+    t = sum(times) / len(times)
+    value = n_eval / t * world
+    hbm, bf16, peak_src = measured_peaks()
+    kpad = ((n + 255) // 256) * 256
+    ops = 2.0 * kpad * 64 * (N * (N - 1) / 2)
+    cpu = None
+    if not args.no_cpu and reference_binary() and rank == 0:
+        threads = os.cpu_count() or 1
+        with tempfile.TemporaryDirectory() as d:
+            npairs, dt = reference_pairs_run(X, n, U, y, W["cpu_N"], threads, d)
+        cpu = {"value": npairs / dt, "unit": "pair tests/s", "cores": threads, "kind": "reference",
+               "sample": f"reference kgwas_2d on {W['cpu_N']} k-mers ({npairs} pairs), n={n}, r={r}+1, "
+                         "wall clock incl. its index load"}
+    line = {"metric": f"pair tests/s (2-D pair test, n={n}, r={r}+1, {N} k-mers)", "value": value,
+            "unit": "pair tests/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "i8 limbs -> i32 TMEM, f64 epilogue", "data": "synthetic (seeded, generated on device)",
+            "config": {"workload": f"pairs: n={n}, N={N} k-mers ({N * (N - 1) // 2} pairs), r={r}+1, "
+                                   "log10_thresh=6", "parallelism": f"weak: {world} GPU(s)"},
+            "pairs_scored": n_eval, "pairs_emitted": int(res.shape[0]),
+            "roofline": {"bound": "tensor", "achieved": ops / t / 1e12, "peak": 2 * bf16, "unit": "TOP/s int8",
+                         "frac": ops / t / 1e12 / (2 * bf16), "peak_source": peak_src + " (2x bf16 burst)",
+                         "traffic": None},
+            "e2e": {"value": value, "unit": "pair tests/s", "h2d_bytes_per_step": int(X.nbytes),
+                    "d2h_bytes_per_step": int(res.shape[0]) * 40 + 32, "api": "kg_pairs_run_host"},
+            "gpu_launches": 2 * args.steps, "clocks": ck.summary(), "cpu_baseline": cpu}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    g.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -541,9 +636,9 @@ def main():
     ap.add_argument("--cpu-kmers", type=int, default=1_000_000)
     ap.add_argument("--ref-kmers", type=int, default=250_000)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="precision", choices=["precision", "batched", "streaming"],
+    ap.add_argument("--workload", default="precision", choices=["precision", "batched", "streaming", "pairs"],
                     help="precision: the default single-phenotype workload; batched: 64 phenotypes; "
-                         "streaming: 8 phenotypes at n=5000 from pinned host memory")
+                         "streaming: 8 phenotypes at n=5000 from pinned host memory; pairs: the 2-D pair test")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours" and not os.environ.get("KG_BENCH_ALLOW_SHORT"):
         args.warmup = 3
@@ -553,6 +648,8 @@ def main():
         run_batched(args)
     elif args.workload == "streaming":
         run_streaming(args)
+    elif args.workload == "pairs":
+        run_pairs(args)
     else:
         run_ours(args)
 

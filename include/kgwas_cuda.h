@@ -192,6 +192,38 @@ int kg_fetch_multi(kg_ctx* ctx, kg_multi_result* res);
 int kg_run_multi_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t n_kmers, uint32_t words_per_kmer,
                       const uint64_t* shard_start, int n_shards, kg_multi_result* res);
 
+/* ---------------------------------------------------------------------
+ * 2-D pair test (the reference's kgwas_2d, src/kgwas_2d.cpp:210-392).
+ *
+ * For every pair i < j of the n_kmers packed rows with row_start <= i <
+ * row_end (the reference's --task-id/--num-tasks row range, :245-250), the
+ * column x_i * x_j (AND of the rows) is tested like one k-mer of the 1-D
+ * test against the structure and phenotype of kg_set_structure, without the
+ * Pearson pre-filter: pairs with popcount(x_i * x_j) = 0, xxM <= 1e-12 or
+ * yyM <= 1e-12 are skipped (:292-304), and pairs with p <= 10^-log10_thresh
+ * are returned (:306-318).  Split precision only; every returned pair is
+ * recomputed in FP64.
+ * ------------------------------------------------------------------- */
+typedef struct kg_pair {
+    uint64_t a, b;      /* k-mer indices, a < b                               */
+    double effect;      /* xyM / (xxM * yyM)                                  */
+    double pval;        /* erfc(sqrt(T/2))                                    */
+    double chisq;       /* T = n ln(1/(1 - r^2))                              */
+} kg_pair;
+
+typedef struct kg_pair_result {
+    uint64_t n_kmers;
+    uint64_t n_evaluated; /* pairs that received a p-value                  */
+    uint64_t n_pairs;     /* pairs with p <= 10^-log10_thresh               */
+    const kg_pair* pairs; /* sorted by (a, b); owned by the context, valid until
+                             the next call on it                              */
+} kg_pair_result;
+
+/* Replaces build_stats2d_self + emit_pairs_self (src/kgwas_2d.cpp:210-392).
+ * xbits: host rows as for kg_run_host; n_kmers < 2^32. */
+int kg_pairs_run_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t n_kmers, uint32_t words_per_kmer,
+                      uint64_t row_start, uint64_t row_end, kg_pair_result* res);
+
 /* Number of kernel launches the last kg_run_host / kg_launch_device made. */
 int kg_last_launch_count(const kg_ctx* ctx);
 

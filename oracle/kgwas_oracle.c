@@ -153,3 +153,63 @@ int64_t kgo_cols(const uint64_t* x, int64_t m, int wpk, int n,
 void kgo_mlog10p(const double* T, int64_t m, double* out) {
     for (int64_t j = 0; j < m; ++j) out[j] = mlog10_chi2_sf_k1(T[j]);
 }
+
+/*
+ * 2-D pair test (src/kgwas_2d.cpp:237-331, emit_pairs_self): for every pair
+ * i < j of k-mers with row_start <= i < row_end, the column x12 = x_i * x_j
+ * (AND of the packed rows) goes through the same low-rank statistic as one
+ * k-mer of the 1-D test, without the Pearson pre-filter:
+ *   a33 = popcount(x12) must be > 0 (this implies a11, a22 > 0);
+ *   xxM = a33 - ||U^T x12||^2, xyM = x12.y - (U^T x12).(U^T y);
+ *   compute_hit (src/kgwas.cpp:44-56).
+ * The reference evaluates x12.y and U^T x12 in FP32 (src/kgwas_2d.cpp:306-312);
+ * here in long double.  Outputs are dense N x N arrays indexed i*N + j (only
+ * i < j inside the row range are written); evaluated[i*N+j] = 1 when a33 > 0,
+ * xxM > eps and yyM > eps, the pairs the reference gives a p-value (the
+ * others are skipped, src/kgwas_2d.cpp:300-313).  Returns their number.
+ */
+int64_t kgo_pairs(const uint64_t* x, int64_t N, int wpk, int n, const double* U, int k, const double* y,
+                  int64_t row_start, int64_t row_end, uint8_t* evaluated, double* T_out, double* p_out,
+                  double* eff_out, double* ml_out) {
+    double* Uy = (double*)malloc(sizeof(double) * (size_t)(k > 0 ? k : 1));
+    const double yyM = kgo_yyM(n, U, k, y, Uy);
+    ld* Ux = (ld*)malloc(sizeof(ld) * (size_t)(k > 0 ? k : 1));
+    uint64_t* w12 = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)wpk);
+    int64_t n_eval = 0;
+    if (row_end > N) row_end = N;
+    for (int64_t i = row_start; i < row_end; ++i) {
+        const uint64_t* xi = x + (size_t)i * wpk;
+        for (int64_t j = i + 1; j < N; ++j) {
+            const uint64_t* xj = x + (size_t)j * wpk;
+            int c = 0;
+            for (int w = 0; w < wpk; ++w) { w12[w] = xi[w] & xj[w]; c += __builtin_popcountll(w12[w]); }
+            const size_t o = (size_t)i * (size_t)N + (size_t)j;
+            double eff = 0, T = 0, p = 1, ml = 0;
+            int ev = 0;
+            if (c > 0) {
+                for (int t = 0; t < k; ++t) Ux[t] = 0;
+                ld xdy = 0;
+                for (int s = 0; s < n; ++s) {
+                    if (!((w12[s >> 6] >> (s & 63)) & 1u)) continue;
+                    xdy += y[s];
+                    for (int t = 0; t < k; ++t) Ux[t] += U[(size_t)t * n + s];
+                }
+                ld sUX = 0, UyUX = 0;
+                for (int t = 0; t < k; ++t) { sUX += Ux[t] * Ux[t]; UyUX += Ux[t] * (ld)Uy[t]; }
+                const double xxM = (double)((ld)c - sUX);
+                const double xyM = (double)(xdy - UyUX);
+                ev = xxM > 1e-12 && yyM > 1e-12;
+                n_eval += ev;
+                compute_hit(xxM, xyM, yyM, n, &eff, &T, &p);
+                ml = mlog10_chi2_sf_k1(T);
+            }
+            if (evaluated) evaluated[o] = (uint8_t)ev;
+            if (T_out) T_out[o] = T;
+            if (p_out) p_out[o] = p;
+            if (eff_out) eff_out[o] = eff;
+            if (ml_out) ml_out[o] = ml;
+        }
+    }
+    free(w12); free(Ux); free(Uy);
+    return n_eval;
+}

@@ -1,5 +1,5 @@
 #!/usr/bin/env bash
-# Stage the reference's shipped kgwas binary into oracle/_ref/ so that it can
+# Stage the reference's shipped kgwas, kgwas_2d and build_index binaries into oracle/_ref/ so that it can
 # be RUN as a black box (CPU baseline and golden-vector generation).  The
 # reference cannot be rebuilt from source here: src/kgwas.cpp includes
 # <Eigen/Dense> and links OpenBLAS, neither of which is installed.  The binary
@@ -17,6 +17,10 @@ if [[ ! -x "$REF/bin/kgwas" ]]; then
 fi
 mkdir -p "$OUT"
 cp -f "$REF/bin/kgwas" "$OUT/kgwas"
+# the 2-D pair test and the index builder that produces its input
+for b in kgwas_2d build_index; do
+  [[ -x "$REF/bin/$b" ]] && cp -f "$REF/bin/$b" "$OUT/$b"
+done
 PY="$(command -v python3)"
 LIBS="$("$PY" -c 'import os,glob,sys; d=[p for p in sys.path if p.endswith("site-packages")]; g=[x for s in d for x in glob.glob(os.path.join(s,"opencv_python_headless.libs"))]; print(g[0] if g else "")')"
 if [[ -n "$LIBS" ]]; then

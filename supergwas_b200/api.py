@@ -70,6 +70,15 @@ class _MultiResult(ctypes.Structure):
                 ("n_tested", ctypes.POINTER(ctypes.c_uint64)), ("n_hits", ctypes.c_uint64),
                 ("hits", ctypes.c_void_p)]
 
+PAIR_DTYPE = np.dtype([("a", np.uint64), ("b", np.uint64), ("effect", np.float64), ("pval", np.float64),
+                       ("chisq", np.float64)])
+
+
+class _PairResult(ctypes.Structure):
+    _fields_ = [("n_kmers", ctypes.c_uint64), ("n_evaluated", ctypes.c_uint64), ("n_pairs", ctypes.c_uint64),
+                ("pairs", ctypes.c_void_p)]
+
+
 _LIB = None
 
 
@@ -117,6 +126,8 @@ def lib():
     L.kg_fetch_multi.argtypes = [vp, ctypes.POINTER(_MultiResult)]
     L.kg_run_multi_host.argtypes = [vp, vp, ctypes.c_uint64, ctypes.c_uint32, vp, ctypes.c_int,
                                     ctypes.POINTER(_MultiResult)]
+    L.kg_pairs_run_host.argtypes = [vp, vp, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64,
+                                    ctypes.POINTER(_PairResult)]
     L.kg_run_device_noalloc.argtypes = [vp, ctypes.c_uint64, ctypes.c_uint32, _DP, ctypes.c_int, ctypes.c_int,
                                         _DP, ctypes.c_double, ctypes.c_double, vp, ctypes.c_uint64,
                                         ctypes.POINTER(ctypes.c_uint64), vp, ctypes.c_char_p, ctypes.c_size_t]
@@ -247,6 +258,21 @@ class Kgwas:
         self._check(self._L.kg_fetch(self._h, ctypes.byref(r), ctypes.byref(st) if st is not None else None),
                     "kg_fetch")
         return self._result(r, arrs)
+
+    # ------------------------------------------------------ 2-D pair test
+    def run_pairs_host(self, packed: np.ndarray, row_start: int = 0, row_end: int | None = None):
+        """Pairs i < j with row_start <= i < row_end and p <= 10^-log10_thresh,
+        sorted by (a, b): (PAIR_DTYPE array, number of pairs scored)."""
+        packed = np.ascontiguousarray(packed, dtype=np.uint64)
+        m, wpk = packed.shape
+        r = _PairResult()
+        self._check(self._L.kg_pairs_run_host(self._h, packed.ctypes.data, m, wpk, row_start,
+                                              m if row_end is None else row_end, ctypes.byref(r)),
+                    "kg_pairs_run_host")
+        out = np.zeros(r.n_pairs, PAIR_DTYPE)
+        if r.n_pairs:
+            ctypes.memmove(out.ctypes.data, r.pairs, r.n_pairs * PAIR_DTYPE.itemsize)
+        return out, int(r.n_evaluated)
 
     # ---------------------------------------------------- many phenotypes
     def set_phenotypes(self, phenos, n_row_samples: int):

@@ -3,6 +3,7 @@
 Outputs (git-ignored, shipped with the source tree):
   supergwas_b200/lib/libkgwas_cuda.so   C ABI of include/kgwas_cuda.h
   supergwas_b200/bin/kgwas              drop-in for the reference's kgwas CLI
+  supergwas_b200/bin/kgwas_2d           drop-in for the reference's kgwas_2d CLI
 
 Everything device-side is compiled for sm_100a only.
 """
@@ -21,11 +22,13 @@ LIB_DIR = os.path.join(PKG, "lib")
 BIN_DIR = os.path.join(PKG, "bin")
 LIB = os.path.join(LIB_DIR, "libkgwas_cuda.so")
 CLI = os.path.join(BIN_DIR, "kgwas")
+CLI2 = os.path.join(BIN_DIR, "kgwas_2d")
 OBJ_DIR = os.path.join(PKG, "_build")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-LIB_SOURCES = ["kernels.cu", "kernel_ts.cu", "kernel_mp.cu", "kernel_mpb.cu", "noalloc.cu", "capi.cpp", "capi_multi.cpp", "prep.cpp"]
+LIB_SOURCES = ["kernels.cu", "kernel_ts.cu", "kernel_mp.cu", "kernel_mpb.cu", "kernel_pairs.cu", "capi_pairs.cpp", "noalloc.cu", "capi.cpp", "capi_multi.cpp", "prep.cpp"]
 CLI_SOURCES = ["kgwas_main.cpp", "kgwas_io.cpp"]
+CLI2_SOURCES = ["kgwas2d_main.cpp", "kgwas_io.cpp"]
 
 
 def nvcc() -> str:
@@ -81,21 +84,24 @@ def build_lib(force=False, verbose=False, ptxas_verbose=False) -> str:
     return LIB
 
 
-def build_cli(force=False, verbose=False) -> str:
-    deps = _deps(CLI_SOURCES) + [LIB]
-    if not force and _newer(CLI, deps):
-        return CLI
+def build_cli(force=False, verbose=False, target=None, sources=None) -> str:
+    target = target or CLI
+    sources = sources or CLI_SOURCES
+    deps = _deps(sources) + [LIB]
+    if not force and _newer(target, deps):
+        return target
     os.makedirs(BIN_DIR, exist_ok=True)
-    cmd = ["g++", "-O3", "-std=c++17", "-fopenmp", "-o", CLI,
-           *[os.path.join(CSRC, s) for s in CLI_SOURCES],
+    cmd = ["g++", "-O3", "-std=c++17", "-fopenmp", "-o", target,
+           *[os.path.join(CSRC, s) for s in sources],
            "-L" + LIB_DIR, "-lkgwas_cuda", "-Wl,-rpath,$ORIGIN/../lib", "-lz", "-lpthread"]
     run(cmd, verbose)
-    return CLI
+    return target
 
 
 def build_all(force=False, verbose=False):
     build_lib(force, verbose)
     build_cli(force, verbose)
+    build_cli(force, verbose, CLI2, CLI2_SOURCES)
     return LIB, CLI
 
 

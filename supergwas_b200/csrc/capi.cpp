@@ -93,6 +93,9 @@ void kg_destroy(kg_ctx* ctx) {
   dfree(ctx->dHits);
   dfree(ctx->dCand);
   dfree(ctx->dTested);
+  dfree(ctx->dPX);
+  dfree(ctx->dPairs);
+  dfree(ctx->dUnitOff);
   for (auto& p : ctx->dStat) dfree(p);
   for (int b = 0; b < NBUF; ++b) {
     dfree(ctx->dChunk[b]);
@@ -235,6 +238,9 @@ int ensure_cand(kg_ctx* ctx, unsigned long long cap) {
 int ensure_stats(kg_ctx* ctx, size_t m) {
   if (ctx->stat_cap >= m && ctx->dTested) return KG_OK;
   dfree(ctx->dTested);
+  dfree(ctx->dPX);
+  dfree(ctx->dPairs);
+  dfree(ctx->dUnitOff);
   for (auto& p : ctx->dStat) dfree(p);
   ctx->stat_cap = 0;
   KG_CUDA(cudaMalloc((void**)&ctx->dTested, std::max<size_t>(m, 1)), "cudaMalloc(stats)");

@@ -149,6 +149,14 @@ struct kg_ctx {
   cudaEvent_t ev_h2d[kgctx::NBUF] = {}, ev_k[kgctx::NBUF] = {};
   // many phenotypes
   kgctx::Multi mp;
+  // 2-D pair test
+  uint64_t* dPX = nullptr;        // packed rows on the device
+  size_t px_bytes = 0;
+  kg_pair* dPairs = nullptr;
+  unsigned long long pair_cap = 0;
+  unsigned long long* dUnitOff = nullptr;
+  size_t unit_cap = 0;
+  std::vector<kg_pair> pairs;
 
   int fail(int code, const std::string& m) {
     err = m;

@@ -127,6 +127,32 @@ size_t mpb_smem_bytes(int N, int kpad);
 cudaError_t launch_mpb(const LaunchMpb& L, cudaStream_t st);
 cudaError_t launch_mp_refine(const LaunchMpRefine& L, cudaStream_t st);
 
+// 2-D pair test (kernel_pairs.cu): the TMEM-A pipeline on x_i AND x_j.
+struct LaunchPairs {
+  const uint64_t* x;          // packed rows (device), 16-byte aligned, wpk >= 16
+  int wpk;
+  int kpad;
+  bool drop0;
+  PairSched S;
+  const int8_t* Bimg;         // make_b_image_ts layout (device)
+  const EpiParams* P;
+  const LimbMap* LM;
+  const DevOutPairs* O;
+  int num_sms;
+};
+struct LaunchPairRefine {
+  const uint64_t* x;
+  int wpk;
+  const double* T;            // byte tables of V (refine_table_len(vrows, cm) doubles)
+  int vrows, cm;
+  const EpiParams* P;
+  const DevOutPairs* O;
+  int num_sms;
+};
+bool pairs_supported(int N, int limbs_u, int limbs_y, int kpad, int wpk);
+cudaError_t launch_pairs(const LaunchPairs& L, cudaStream_t st);
+cudaError_t launch_pair_refine(const LaunchPairRefine& L, cudaStream_t st);
+
 int tc_kc();                  // samples per K chunk of the tensor-core kernel
 bool tc_supported_n(int N);
 cudaError_t launch_tc(const LaunchTc& L, cudaStream_t st);

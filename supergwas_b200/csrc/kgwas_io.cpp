@@ -421,4 +421,171 @@ size_t RowsReader::read(size_t max_rows, const std::vector<int>& idxs, std::vect
   return got;
 }
 
+// ------------------------------------------------ sharded index (2-D input)
+
+namespace {
+
+using Key = unsigned __int128;
+
+bool read_meta(const std::string& dir, uint32_t& K, uint32_t& M, uint64_t& N) {
+  std::ifstream in(dir + "/index.meta");
+  if (!in) {
+    std::cerr << "[ERROR] cannot read index.meta in " << dir << "\n";
+    return false;
+  }
+  std::string line;
+  K = 0;
+  M = 0;
+  N = 0;
+  while (std::getline(in, line)) {
+    if (line.compare(0, 2, "K=") == 0) K = (uint32_t)std::stoul(line.substr(2));
+    else if (line.compare(0, 2, "M=") == 0) M = (uint32_t)std::stoul(line.substr(2));
+    else if (line.compare(0, 2, "N=") == 0) N = std::stoull(line.substr(2));
+  }
+  if (K == 0 || M == 0) {
+    std::cerr << "[ERROR] invalid index.meta (K=" << K << " M=" << M << ")\n";
+    return false;
+  }
+  return true;
+}
+
+bool slurp(const std::string& path, std::vector<char>& buf, const char* what) {
+  std::ifstream in(path, std::ios::binary);
+  if (!in) {
+    std::cerr << "[ERROR] cannot open " << path << "\n";
+    return false;
+  }
+  in.seekg(0, std::ios::end);
+  buf.resize((size_t)in.tellg());
+  in.seekg(0, std::ios::beg);
+  in.read(buf.data(), (std::streamsize)buf.size());
+  if (!in) {
+    std::cerr << "[ERROR] short read: " << path << "\n";
+    return false;
+  }
+  (void)what;
+  return true;
+}
+
+// One shard: the keys of its .umap (first record of a key kept) and, from
+// its .bits, the last non-empty bitstring recorded for each key.
+bool load_shard_bits(const std::string& dir, uint32_t sid, uint32_t K, std::vector<std::pair<Key, std::string>>& out) {
+  char fname[32];
+  std::snprintf(fname, sizeof(fname), "shard_%03u", sid);
+  const std::string umap = dir + "/" + fname + ".umap", bitsp = dir + "/" + fname + ".bits";
+  std::vector<char> buf;
+  if (!slurp(umap, buf, "umap")) return false;
+  if (buf.size() < 20) {
+    std::cerr << "[ERROR] file too small: " << umap << "\n";
+    return false;
+  }
+  static const char MAGIC[8] = {'U', 'M', 'A', 'P', 'd', '4', '\0', '\0'};
+  if (std::memcmp(buf.data(), MAGIC, 8) != 0) {
+    std::cerr << "[ERROR] bad magic in " << umap << "\n";
+    return false;
+  }
+  uint32_t k;
+  uint64_t n;
+  std::memcpy(&k, buf.data() + 8, 4);
+  std::memcpy(&n, buf.data() + 12, 8);
+  if (K && k != K) {
+    std::cerr << "[ERROR] K mismatch in " << umap << ": got " << k << " expected " << K << "\n";
+    return false;
+  }
+  if (buf.size() < 20 + (size_t)n * 32) {
+    std::cerr << "[ERROR] short read: " << umap << "\n";
+    return false;
+  }
+  std::unordered_map<uint64_t, std::vector<size_t>> seen;  // hash of key -> slots
+  std::vector<Key> keys;
+  std::vector<std::string> bits;
+  auto hkey = [](Key x) { return (uint64_t)x ^ (uint64_t)(x >> 64) * 0x9E3779B97F4A7C15ull; };
+  auto find = [&](Key x) -> long {
+    auto it = seen.find(hkey(x));
+    if (it == seen.end()) return -1;
+    for (size_t s : it->second)
+      if (keys[s] == x) return (long)s;
+    return -1;
+  };
+  std::vector<Key> rec((size_t)n);
+  for (uint64_t i = 0; i < n; ++i) {
+    Key x;
+    std::memcpy(&x, buf.data() + 20 + i * 32, 16);
+    rec[i] = x;
+    if (find(x) < 0) {
+      seen[hkey(x)].push_back(keys.size());
+      keys.push_back(x);
+      bits.emplace_back();
+    }
+  }
+  std::vector<char> bb;
+  if (!slurp(bitsp, bb, "bits")) return false;
+  if (bb.size() < 8) {
+    std::cerr << "[ERROR] short read: " << bitsp << "\n";
+    return false;
+  }
+  uint64_t bn;
+  std::memcpy(&bn, bb.data(), 8);
+  if (bn != n) {
+    std::cerr << "[ERROR] .bits N=" << bn << " != .umap N=" << n << "\n";
+    return false;
+  }
+  size_t off = 8;
+  for (uint64_t i = 0; i < n; ++i) {
+    uint32_t blen = 0;
+    if (off + 4 > bb.size()) return false;
+    std::memcpy(&blen, bb.data() + off, 4);
+    off += 4;
+    if (blen > 0) {
+      if (off + blen > bb.size()) return false;
+      const long s = find(rec[i]);
+      if (s >= 0) bits[(size_t)s].assign(bb.data() + off, blen);
+    }
+    off += blen;
+  }
+  for (size_t s = 0; s < keys.size(); ++s)
+    if (!bits[s].empty()) out.emplace_back(keys[s], std::move(bits[s]));
+  return true;
+}
+
+}  // namespace
+
+IndexBits load_index_bits(const std::string& dir, int threads) {
+  Timer t;
+  struct stat st;
+  if (stat(dir.c_str(), &st) != 0 || !S_ISDIR(st.st_mode)) die("Index path is not a directory: " + dir);
+  uint32_t K = 0, M = 0;
+  uint64_t N = 0;
+  if (!read_meta(dir, K, M, N)) die("Failed to read index meta from " + dir);
+  std::vector<std::vector<std::pair<Key, std::string>>> shards(M);
+  std::atomic<bool> ok{true};
+#pragma omp parallel for schedule(dynamic, 1) num_threads(std::max(1, threads))
+  for (int64_t s = 0; s < (int64_t)M; ++s)
+    if (!load_shard_bits(dir, (uint32_t)s, K, shards[(size_t)s])) ok = false;
+  if (!ok) die("Failed to load index shards");
+  std::vector<std::pair<Key, std::string>> all;
+  for (auto& v : shards)
+    for (auto& e : v) all.push_back(std::move(e));
+  std::cerr << "[INFO] Loaded index: " << all.size() << " kmers with bitstrings (" << M << " shards, K=" << K
+            << ") in " << t.sec() << " s\n";
+  std::sort(all.begin(), all.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+  if (all.empty()) die("No k-mers with bitstrings in index");
+  IndexBits out;
+  out.K = K;
+  out.kmers.resize(all.size());
+  out.bits.resize(all.size());
+  static const char DEC[4] = {'A', 'C', 'G', 'T'};
+  for (size_t i = 0; i < all.size(); ++i) {
+    std::string& s = out.kmers[i];
+    s.resize(K);
+    Key e = all[i].first;
+    for (uint32_t c = K; c > 0; --c) {
+      s[c - 1] = DEC[(unsigned)(e & 3u)];
+      e >>= 2;
+    }
+    out.bits[i] = std::move(all[i].second);
+  }
+  return out;
+}
+
 }  // namespace kgio

@@ -68,4 +68,20 @@ struct RowsReader {
   bool next_line(std::string& line);
 };
 
+// Sharded k-mer index with bitstrings (the input of the 2-D pair test):
+// INDEX_DIR/index.meta ("K=", "M=", "N=" lines) and, per shard s < M,
+// shard_%03u.umap (magic "UMAPd4\0\0", uint32 K, uint64 N, N records of a
+// 16-byte 2-bit-encoded canonical k-mer + FP64 effect + FP64 p) and
+// shard_%03u.bits (uint64 N, then per record uint32 length + bitstring).
+// Follows load_X_from_index (src/kgwas_2d.cpp:80-153) and read_index_meta /
+// load_shard (src/map_utils.hpp:319-479): the k-mers that carry a bitstring,
+// sorted by their encoding, decoded to A/C/G/T.  Failures print the
+// reference's [ERROR] lines and exit(1).
+struct IndexBits {
+  uint32_t K = 0;
+  std::vector<std::string> kmers;
+  std::vector<std::string> bits;
+};
+IndexBits load_index_bits(const std::string& dir, int threads);
+
 }  // namespace kgio

@@ -83,4 +83,22 @@ struct DevOutMP {
   unsigned long long kmer_offset;
 };
 
+// Outputs of the 2-D pair test (kernel_pairs.cu).
+struct DevOutPairs {
+  unsigned long long* counters;  // [0] evaluated pairs, [1] hits, [2] error bits, [3] refinement candidates
+  kg_pair* hits;
+  unsigned long long hit_cap;
+  unsigned long long* cand;      // i << 32 | j
+  unsigned long long cand_cap;
+};
+
+// Pair schedule: pairs (i, j), i < j, row_start <= i < row_end, j < n_kmers.
+// Unit u covers j-block jb (j in [128 jb, 128 jb + 128)) and up to `ic`
+// consecutive i; units of j-block jb are unit_off[jb] .. unit_off[jb+1]-1.
+struct PairSched {
+  const unsigned long long* unit_off;  // njb + 1 entries (device)
+  int njb;
+  unsigned long long n_units, n_kmers, row_start, row_end, ic;
+};
+
 }  // namespace kg

@@ -380,13 +380,103 @@ def make_faults():
 
 FIXTURES = {"small": fx_small, "edge": fx_edge, "yspan": fx_yspan}
 
+
+# ------------------------------------------------------------ 2-D pair test
+
+PAIR_VARIANTS = [
+    {"name": "l0", "args": ["0"]},                                # every scored pair is a row
+    {"name": "l2", "args": ["2"]},
+    {"name": "task1of3", "args": ["1.5", "--num-tasks", "3", "--task-id", "1"]},
+    {"name": "task5of3", "args": ["1.5", "--num-tasks", "3", "--task-id", "5"]},  # no rows
+]
+
+
+def make_pairs():
+    """2-D pair test (src/kgwas_2d.cpp): a kgwas-style .2d.tsv of k-mers with
+    bitstrings is turned into a sharded index by the reference's build_index
+    and tested by the reference's kgwas_2d; inputs (index directory included)
+    and outputs are committed.  Edge cases of the index reader: bitstrings of
+    the overlap length and of the samples length, bitstrings of another
+    length (dropped), rows without a bitstring (not in the test), a k-mer and
+    its reverse complement (one canonical entry), an all-zero and an all-one
+    row."""
+    rng = np.random.default_rng(29)
+    n_all, m = 110, 160
+    pop = (np.arange(n_all) * 3) // n_all
+    _, ps = synth.draw_frequencies(rng, m, 3)
+    x = synth.draw_bits(rng, ps, pop)
+    x[4, :] = 0
+    x[5, :] = 1
+    miss = np.sort(rng.choice(n_all, size=7, replace=False))
+    keep = np.setdiff1d(np.arange(n_all), miss)
+    n = keep.size
+    X = x[:, keep].astype(float)
+    y = 1.5 * X[10] * X[20] - 1.0 * X[30] * X[40] + rng.standard_normal(n)
+    Q, _ = np.linalg.qr(np.column_stack([np.ones(n), X[rng.choice(m, 40)].T @ rng.standard_normal((40, 3))]))
+    kmers = synth.random_kmers(rng, m, 31)
+    comp = {"A": "T", "C": "G", "G": "C", "T": "A"}
+    kmers[7] = "".join(comp[c] for c in reversed(kmers[6]))     # reverse complement of k-mer 6
+    samples = [f"s{i:03d}" for i in range(n_all)]
+    fx_dir = os.path.join(HERE, "pairs")
+    os.makedirs(fx_dir, exist_ok=True)
+    with open(os.path.join(fx_dir, "samples.txt"), "w") as f:
+        f.write("".join(s + "\n" for s in samples))
+    with open(os.path.join(fx_dir, "phenotype.txt"), "w") as f:
+        f.write("".join(f"{samples[i]}\t{float(v)!r}\n" for i, v in zip(keep, y)))
+    np.savez_compressed(os.path.join(fx_dir, "inputs.npz"), U=Q, y=y, idxs=keep.astype(np.int64),
+                        n_all=np.int64(n_all))
+    lines = []
+    for j in range(m):
+        if j in (11, 12):                                       # no bitstring
+            lines.append(f"{kmers[j]}\t0.1\t1e-30\n")
+            continue
+        if j in (13, 14):                                       # wrong length: dropped
+            b = "".join("1" if v else "0" for v in x[j, keep[:-3]])
+        elif j % 9 == 0:                                        # samples order (length n_all)
+            b = "".join("1" if v else "0" for v in x[j])
+        else:                                                   # overlap order (length n)
+            b = "".join("1" if v else "0" for v in x[j, keep])
+        lines.append(f"{kmers[j]}\t{b}\t0.1\t1e-30\n")
+    work = tempfile.mkdtemp()
+    tsv = os.path.join(work, "hits.2d.tsv")
+    with open(tsv, "w") as f:
+        f.write("kmer\tbits\teffect\tp_value\n" + "".join(lines))
+    idx = os.path.join(fx_dir, "index")
+    if os.path.isdir(idx):
+        shutil.rmtree(idx)
+    r = O.run_reference_tool("build_index", [tsv, idx, "--shards", "4"])
+    assert r.returncode == 0, r.stderr
+    for f in os.listdir(idx):
+        if f.endswith(".bloom"):
+            os.remove(os.path.join(idx, f))                     # not read by kgwas_2d
+    synth.write_ubin(os.path.join(work, "U2D.bin"), Q)
+    meta = {"desc": "2-D pair test: n_all=110 (103 phenotyped), 160 k-mers (2 without bitstrings, 2 with a "
+                    "bitstring of another length, one reverse-complement duplicate), r=3+1, two planted pairs",
+            "variants": PAIR_VARIANTS}
+    with open(os.path.join(fx_dir, "meta.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+    for v in PAIR_VARIANTS:
+        out = os.path.join(work, "out_" + v["name"])
+        r = O.run_reference_tool("kgwas_2d", [os.path.join(fx_dir, "samples.txt"), os.path.join(fx_dir, "phenotype.txt"),
+                                              os.path.join(work, "U2D.bin"), idx, out, *v["args"]],
+                                 {"BLAS_THREADS": 4, "EMIT_THREADS": 4})
+        tag = "ref_" + v["name"]
+        with open(os.path.join(fx_dir, tag + ".rc"), "w") as f:
+            f.write(f"{r.returncode}\n")
+        for ext in (".tsv", ".part_1.tsv", ".part_5.tsv", ".kmers"):
+            if os.path.exists(out + ext):
+                shutil.copy(out + ext, os.path.join(fx_dir, tag + ext))
+    shutil.rmtree(work)
+
 if __name__ == "__main__":
     if not O.ref_available():
         sys.exit("stage the reference first: bash oracle/stage_ref.sh")
-    names = sys.argv[1:] or [*FIXTURES, "cfg1", "faults"]
+    names = sys.argv[1:] or [*FIXTURES, "cfg1", "faults", "pairs"]
     for nm in names:
         if nm == "cfg1":
             make_cfg1()
+        elif nm == "pairs":
+            make_pairs()
         elif nm == "faults":
             make_faults()
         else:
