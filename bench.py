@@ -575,7 +575,7 @@ def run_pairs(args):
         W["N"] = args.kmers
     n, N, r = W["n"], W["N"], W["r"]
     Xd = synth_gpu.gen_packed(n, N, W["S"], W["seed"] + 1000 * rank)
-    U, _, keep, _ = synth_gpu.structure_and_phenotype(Xd, n, r, 0, 0.0, W["seed"])
+    U, _, keep, _ = synth_gpu.structure_and_phenotype(Xd, n, r, 1, 0.0, W["seed"])
     X = Xd.cpu().numpy().view(np.uint64)
     from supergwas_b200 import synth
     x = synth.unpack_rows(X[:64], n).astype(np.float64)

@@ -79,7 +79,7 @@ __host__ __device__ inline TsSmem ts_smem(int b_bytes, int xst) {
   return L;
 }
 
-template <int N, bool DROP0>
+template <int N, bool DROP0, bool GATE>
 __global__ void __launch_bounds__(ts_threads(N), 1)
     ts_kernel(const __grid_constant__ CUtensorMap tmap, unsigned long long m, int nbox, int nsub, int xst,
               const int8_t* __restrict__ Bimg, int b_bytes, const __grid_constant__ EpiParams P,
@@ -320,15 +320,13 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
          tile += 2ull * gridDim.x, ++jt) {
       if (!__all_sync(0xffffffffu, wait_or_abort(acc_full + 8 * e, jt & 1u, s_abort, O.counters, ERR_TIMEOUT_MMA))) break;
       tc_fence_after();
+      // all N columns in flight at once, then one wait
       uint32_t d[N];
 #pragma unroll
-      for (int c16 = 0; c16 < N / 16; ++c16) {
-        uint32_t rr[16];
-        tc_ld16(tmem + lane_base + e * N + c16 * 16, rr);
-        tc_wait_ld();
+      for (int c16 = 0; c16 < N / 16; ++c16) tc_ld16p(tmem + lane_base + e * N + c16 * 16, d + c16 * 16);
+      tc_wait_ld();
 #pragma unroll
-        for (int k = 0; k < 16; ++k) d[c16 * 16 + k] = rr[k];
-      }
+      for (int c16 = 0; c16 < N / 16; ++c16) reg_fence16(d + c16 * 16);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(acc_empty + 8 * e);
@@ -369,7 +367,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
         const double e = fma(__longlong_as_double(Vb), LM.esc[j], LM.eoff[j]);
         const double sj = fma(P.a[j], cd, e);
         ss = fma(sj, sj, ss);
-        gs = fma(P.g[j], e, gs);
+        if (GATE) gs = fma(P.g[j], e, gs);  // only the Pearson gate reads gs
       }
       if (O.tested) finish_kmer(P, O, local, valid, c, ss, gs, ey);
       else finish_kmer_lean(P, O, local, valid, c, cd, ss, gs, ey, tested_local);
@@ -419,20 +417,21 @@ static int ts_ring_depth(int b_bytes) {
   return x;
 }
 
-template <int N, bool D0>
+template <int N, bool D0, bool GATE>
 static cudaError_t launch_ts_t(const LaunchTs& L, const CUtensorMap& tm, cudaStream_t st) {
   const int b_bytes = L.kpad * N;
   const int xst = ts_ring_depth(b_bytes);
   const size_t smem = ts_smem(b_bytes, xst).total + 1024;
-  cudaError_t e = cudaFuncSetAttribute(ts_kernel<N, D0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e =
+      cudaFuncSetAttribute(ts_kernel<N, D0, GATE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const unsigned long long tiles = (L.m + TS_TM - 1) / TS_TM;
   unsigned long long grid = (unsigned long long)L.num_sms;
   if (grid > tiles) grid = tiles;
   const int nbox = (L.wpk * 8 + 127) / 128;
   const int nsub = L.kpad / TS_KS;
-  ts_kernel<N, D0><<<(unsigned)grid, ts_threads(N), smem, st>>>(tm, L.m, nbox, nsub, xst, L.Bimg, b_bytes, *L.P,
-                                                             *L.LM, *L.O);
+  ts_kernel<N, D0, GATE><<<(unsigned)grid, ts_threads(N), smem, st>>>(tm, L.m, nbox, nsub, xst, L.Bimg, b_bytes,
+                                                                   *L.P, *L.LM, *L.O);
   return cudaGetLastError();
 }
 
@@ -450,9 +449,13 @@ cudaError_t launch_ts(const LaunchTs& L, cudaStream_t st) {
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
   const bool d0 = L.drop0;
+  // the per-k-mer statistics path (O.tested) evaluates the correlation too
+  const bool gate = L.P->corr_thr > 0.0 || L.O->tested != nullptr;
   switch (L.LM->N) {
-#define KG_TS_CASE(NN) \
-  case NN: return d0 ? launch_ts_t<NN, true>(L, tm, st) : launch_ts_t<NN, false>(L, tm, st);
+#define KG_TS_CASE(NN)                                                                       \
+  case NN:                                                                                   \
+    if (gate) return d0 ? launch_ts_t<NN, true, true>(L, tm, st) : launch_ts_t<NN, false, true>(L, tm, st); \
+    return d0 ? launch_ts_t<NN, true, false>(L, tm, st) : launch_ts_t<NN, false, false>(L, tm, st);
     KG_TS_CASE(16)
     KG_TS_CASE(32)
     KG_TS_CASE(48)
