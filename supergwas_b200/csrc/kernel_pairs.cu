@@ -297,18 +297,28 @@ __global__ void __launch_bounds__(pr_threads(N), 1)
             }
             const uint32_t xrow = sx + bslot[bx] * PR_XBYTES + r * 128;
             const uint32_t a_t = tmem + lane_base + A0 + ar.slot * 128;
-            for (int sub = kc; sub < ke; ++sub) {
+            // the super-stage's chunks of row i (uniform across the warp) and
+            // of the j rows, all loads in flight before the first use
+            uint4 wi[PR_SUPER], wj[PR_SUPER];
+#pragma unroll
+            for (int s4 = 0; s4 < PR_SUPER; ++s4) {
+              const int sub = kc + s4;
+              wi[s4] = (sub < ke && sub < half_row) ? __ldg(xi + sub) : make_uint4(0u, 0u, 0u, 0u);
               const int c = sub - bx * (PR_BOX / PR_KS);
-              uint4 w;
-              asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];"
-                           : "=r"(w.x), "=r"(w.y), "=r"(w.z), "=r"(w.w)
-                           : "r"(xrow + ((c ^ (r & 7)) << 4)));
-              // the same 128 samples of row i (uniform across the warp)
-              const uint4 wi = sub < half_row ? __ldg(xi + sub) : make_uint4(0u, 0u, 0u, 0u);
-              const uint32_t w4[4] = {w.x & wi.x, w.y & wi.y, w.z & wi.z, w.w & wi.w};
-              uint32_t o[32];
-              unpack_stage(w4, o);
-              tc_st32(a_t + (sub - kc) * 32, o);
+              if (sub < ke)
+                asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];"
+                             : "=r"(wj[s4].x), "=r"(wj[s4].y), "=r"(wj[s4].z), "=r"(wj[s4].w)
+                             : "r"(xrow + ((c ^ (r & 7)) << 4)));
+            }
+#pragma unroll
+            for (int s4 = 0; s4 < PR_SUPER; ++s4) {
+              if (kc + s4 < ke) {
+                const uint32_t w4[4] = {wj[s4].x & wi[s4].x, wj[s4].y & wi[s4].y, wj[s4].z & wi[s4].z,
+                                        wj[s4].w & wi[s4].w};
+                uint32_t o[32];
+                unpack_stage(w4, o);
+                tc_st32(a_t + s4 * 32, o);
+              }
             }
             kc = ke;
             tc_wait_st();

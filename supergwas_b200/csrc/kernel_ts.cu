@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
     RingN xr(xst);
     Ring<NSLOT> ar;
-    uint32_t turn = 0;  // super-stage counter parity
+    uint32_t turn = 0;  // super-stage counter modulo UG
     bool ok = true;
     for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
       int kc = 0;  // sub-stage of the tile
@@ -248,10 +248,10 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
         // super-stages never straddle a box: a box holds two of them
         while (kc < kc1) {
           const int ke = kc + TS_SUPER < kc1 ? kc + TS_SUPER : kc1;
-          if (UG == 2 && turn != (uint32_t)grp) {  // the other group's super-stage
+          if (UG > 1 && turn != (uint32_t)grp) {  // another group's super-stage
             kc = ke;
             ar.next();
-            turn ^= 1u;
+            turn = turn + 1 == (uint32_t)UG ? 0u : turn + 1;
             continue;
           }
           if (ar.used && !__all_sync(0xffffffffu, wait_or_abort(a_empty + 8 * ar.slot, ar.phase ^ 1u, s_abort,
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
           __syncwarp();
           if (lane == 0) mbar_arrive(a_full + 8 * ar.slot);
           ar.next();
-          if (UG == 2) turn ^= 1u;
+          if (UG > 1) turn = turn + 1 == (uint32_t)UG ? 0u : turn + 1;
         }
         if (!ok) break;
         // every unpack warp releases every box, whether or not it read from it
