@@ -113,6 +113,9 @@ int main(int argc, char** argv) {
   if (N <= 0) die("No valid k-mers after bitstring parsing");
   std::cerr << "[INFO] Built X from index (N=" << N << ", n=" << n << ", " << tx.sec() << " s)\n";
 
+  // emit_pairs_self's column check (src/kgwas_2d.cpp:240), made before the
+  // GPU is touched so that the failure needs no device
+  if (N < 2) die("emit_pairs_self: need at least 2 columns");
   // build_stats2d_self + emit_pairs_self (src/kgwas_2d.cpp:210-392) on the GPU
   Gpu g;
   kg_opts o;
@@ -125,7 +128,6 @@ int main(int argc, char** argv) {
   double yyM = 0;
   g.check(kg_set_structure(g.ctx, ud.U.data(), n, ud.k, ov.y.data(), &yyM), "set_structure");
   if (!(yyM > 1e-12)) kgio::warn("yyM ~ 0");
-  if (N < 2) die("emit_pairs_self: need at least 2 columns");
   const int64_t rows_per_task = (N + cfg.num_tasks - 1) / cfg.num_tasks;
   const int64_t row_start = (int64_t)cfg.task_id * rows_per_task;
   const int64_t row_end = std::min(row_start + rows_per_task, N);

@@ -391,6 +391,138 @@ PAIR_VARIANTS = [
 ]
 
 
+def pair_fault_cases():
+    """(name, mutate(work) -> argv, env) for malformed inputs of kgwas_2d: the
+    checks of parse_args, build_overlap, load_Ubin and load_X_from_index
+    (src/kgwas_2d.cpp:45-207, src/map_utils.hpp:319-479)."""
+    import struct
+
+    def base(w, *extra):
+        return [w["samples"], w["pheno"], w["ubin"], w["index"], w["out"], *extra]
+
+    def shard(w, s, ext):
+        return os.path.join(w["index"], f"shard_{s:03d}{ext}")
+
+    def patch(path, off, data):
+        b = bytearray(open(path, "rb").read())
+        b[off:off + len(data)] = data
+        open(path, "wb").write(bytes(b))
+
+    def rewrite_bits(w, fn):
+        """fn(bitstring) -> new bitstring (or "") for every record of every shard."""
+        meta = open(os.path.join(w["index"], "index.meta")).read()
+        M = int([l for l in meta.splitlines() if l.startswith("M=")][0][2:])
+        for s_ in range(M):
+            p = shard(w, s_, ".bits")
+            b = open(p, "rb").read()
+            (n,) = struct.unpack_from("<Q", b, 0)
+            out, off = [struct.pack("<Q", n)], 8
+            for _ in range(n):
+                (ln,) = struct.unpack_from("<I", b, off)
+                nb = fn(b[off + 4: off + 4 + ln].decode()).encode()
+                out.append(struct.pack("<I", len(nb)) + nb)
+                off += 4 + ln
+            open(p, "wb").write(b"".join(out))
+
+    cases = [("usage", lambda w: ["ONLY"], {})]
+    cases.append(("bad_log10", lambda w: base(w, "abc"), {}))
+    cases.append(("index_not_dir", lambda w: [w["samples"], w["pheno"], w["ubin"], w["index"] + "_nope", w["out"]], {}))
+
+    def meta_missing(w):
+        os.remove(os.path.join(w["index"], "index.meta"))
+        return base(w)
+    cases.append(("meta_missing", meta_missing, {}))
+
+    def meta_invalid(w):
+        open(os.path.join(w["index"], "index.meta"), "w").write("K=0\nM=4\nN=10\n")
+        return base(w)
+    cases.append(("meta_invalid", meta_invalid, {}))
+
+    def umap_missing(w):
+        os.remove(shard(w, 1, ".umap"))
+        return base(w)
+    cases.append(("umap_missing", umap_missing, {}))
+
+    def bad_magic(w):
+        patch(shard(w, 2, ".umap"), 0, b"XMAPd4")
+        return base(w)
+    cases.append(("bad_magic", bad_magic, {}))
+
+    def k_mismatch(w):
+        patch(shard(w, 0, ".umap"), 8, struct.pack("<I", 21))
+        return base(w)
+    cases.append(("k_mismatch", k_mismatch, {}))
+
+    def bits_missing(w):
+        os.remove(shard(w, 3, ".bits"))
+        return base(w)
+    cases.append(("bits_missing", bits_missing, {}))
+
+    def bits_n_mismatch(w):
+        (n,) = struct.unpack_from("<Q", open(shard(w, 1, ".bits"), "rb").read(), 0)
+        patch(shard(w, 1, ".bits"), 0, struct.pack("<Q", n + 1))
+        return base(w)
+    cases.append(("bits_n_mismatch", bits_n_mismatch, {}))
+
+    def no_bitstrings(w):
+        rewrite_bits(w, lambda b: "")
+        return base(w)
+    cases.append(("no_bitstrings", no_bitstrings, {}))
+
+    def all_wrong_length(w):
+        rewrite_bits(w, lambda b: b[:20])
+        return base(w)
+    cases.append(("all_wrong_length", all_wrong_length, {}))
+
+    def one_kmer(w):
+        state = {"kept": 0}
+
+        def keep_one(b):
+            if b and not state["kept"]:
+                state["kept"] = 1
+                return b
+            return ""
+        rewrite_bits(w, keep_one)
+        return base(w)
+    cases.append(("one_kmer", one_kmer, {}))
+
+    def ubin_n_mismatch(w):
+        U = synth.read_ubin(w["ubin"])
+        synth.write_ubin(w["ubin"], U[:-1])
+        return base(w)
+    cases.append(("ubin_n_mismatch", ubin_n_mismatch, {}))
+    return cases
+
+
+def pair_fault_workdir():
+    """A writable copy of the pairs fixture: samples, phenotype, U2D.bin, index."""
+    work = tempfile.mkdtemp()
+    fx = os.path.join(HERE, "pairs")
+    w = {"samples": os.path.join(work, "samples.txt"), "pheno": os.path.join(work, "phenotype.txt"),
+         "ubin": os.path.join(work, "U2D.bin"), "index": os.path.join(work, "index"),
+         "out": os.path.join(work, "out")}
+    shutil.copy(os.path.join(fx, "samples.txt"), w["samples"])
+    shutil.copy(os.path.join(fx, "phenotype.txt"), w["pheno"])
+    shutil.copytree(os.path.join(fx, "index"), w["index"])
+    synth.write_ubin(w["ubin"], np.load(os.path.join(fx, "inputs.npz"))["U"])
+    return work, w
+
+
+def make_pair_faults():
+    out = {}
+    for name, mutate, env in pair_fault_cases():
+        work, w = pair_fault_workdir()
+        argv = mutate(w)
+        e = {"BLAS_THREADS": 1, "EMIT_THREADS": 1}
+        e.update(env)
+        r = O.run_reference_tool("kgwas_2d", argv, e)
+        out[name] = {"rc": r.returncode, "error": error_line(r.stderr, work)}
+        shutil.rmtree(work)
+    with open(os.path.join(HERE, "pair_faults.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    return out
+
+
 def make_pairs():
     """2-D pair test (src/kgwas_2d.cpp): a kgwas-style .2d.tsv of k-mers with
     bitstrings is turned into a sharded index by the reference's build_index
@@ -471,12 +603,14 @@ def make_pairs():
 if __name__ == "__main__":
     if not O.ref_available():
         sys.exit("stage the reference first: bash oracle/stage_ref.sh")
-    names = sys.argv[1:] or [*FIXTURES, "cfg1", "faults", "pairs"]
+    names = sys.argv[1:] or [*FIXTURES, "cfg1", "faults", "pairs", "pair_faults"]
     for nm in names:
         if nm == "cfg1":
             make_cfg1()
         elif nm == "pairs":
             make_pairs()
+        elif nm == "pair_faults":
+            make_pair_faults()
         elif nm == "faults":
             make_faults()
         else:

@@ -192,3 +192,25 @@ def test_cli_errors_match_reference(built):
             assert mg.error_line(r.stderr, work) == exp["error"], (name, r.stderr[-500:])
         finally:
             shutil.rmtree(work)
+
+
+def test_kgwas_2d_errors_match_reference(built):
+    """Malformed kgwas_2d inputs (index directory, shards, bitstrings, U.bin,
+    arguments) give the reference kgwas_2d's exit code and last [ERROR] line,
+    before any GPU work (src/kgwas_2d.cpp:45-207, src/map_utils.hpp:319-479)."""
+    mg = _fault_cases()
+    expected = json.load(open(os.path.join(H.GOLDEN, "pair_faults.json")))
+    exe = os.path.join(build.BIN_DIR, "kgwas_2d")
+    for name, mutate, env in mg.pair_fault_cases():
+        work, w = mg.pair_fault_workdir()
+        try:
+            argv = mutate(w)
+            e = dict(os.environ, BLAS_THREADS="1", EMIT_THREADS="1")
+            e.update({k: str(v) for k, v in env.items()})
+            r = subprocess.run([exe, *argv], capture_output=True, text=True, env=e)
+            exp = expected[name]
+            assert r.returncode == exp["rc"], (name, r.returncode, r.stderr[-500:])
+            assert mg.error_line(r.stderr, work) == exp["error"], (name, r.stderr[-500:])
+        finally:
+            shutil.rmtree(work)
+
