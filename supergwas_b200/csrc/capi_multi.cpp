@@ -480,7 +480,7 @@ int kg_run_multi_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t w
     // Chunks of the rows stream through two device buffers: the copy of
     // chunk i+1 (copy stream) overlaps the kernels of chunk i (compute stream).
     const size_t row = (size_t)wpk * 8;
-    size_t want = (size_t)4096 << 20;
+    size_t want = (size_t)512 << 20;  // small chunks: less copy and compute left unoverlapped at the ends
     if (const char* v = std::getenv("KG_CHUNK_MB")) want = (size_t)std::max(1, std::atoi(v)) << 20;
     uint64_t per = std::max<uint64_t>(1, want / row);
     if (per > m) per = m;
