@@ -344,6 +344,9 @@ def run_ours(args):
         N = 64
         kpad = ((n + 255) // 256) * 256
         tops = 2.0 * m * kpad * N / t_launch / 1e12
+        sm_mhz = clocks.get("sm_mhz") or 0.0
+        n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+        hw_peak = 16384.0 * n_sm * sm_mhz * 1e6 / 1e12 if sm_mhz else None
         acc = accuracy_report(X, min(m, args.acc_kmers), wpk, U, y, keep, n)
         cpu = cpu_baseline(n, r, W["seed"], args.cpu_kmers) if not args.no_cpu else None
         line = {
@@ -362,7 +365,13 @@ def run_ours(args):
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "tensor": {"achieved_tops_int8": tops, "peak_tops_int8": 2 * bf16,
                                     "frac": tops / (2 * bf16),
-                                    "peak_note": "2x measured bf16 burst (int8 MMA issues at twice the bf16 rate)"}},
+                                    "peak_note": "2x measured bf16 burst (int8 MMA issues at twice the bf16 rate)",
+                                    # 16384 int8 ops per SM-cycle at the median SM clock of the timed
+                                    # region; an N=64 MMA reaches 51.6 % of it (bin/mma_rate)
+                                    "hw_peak_tops_int8_at_clock": hw_peak,
+                                    "frac_of_hw_peak": tops / hw_peak if hw_peak else None,
+                                    "n64_mma_ceiling_frac": 0.516,
+                                    "frac_of_n64_ceiling": tops / (0.516 * hw_peak) if hw_peak else None}},
             "fp64_form": {"value": ftested / t_fp64, "unit": "k-mer tests/s", "ms_per_step": 1e3 * t_fp64,
                           "split_speedup": value / world / (ftested / t_fp64)},
             "accuracy_vs_fp64_oracle": acc,
