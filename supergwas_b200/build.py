@@ -23,6 +23,7 @@ BIN_DIR = os.path.join(PKG, "bin")
 LIB = os.path.join(LIB_DIR, "libkgwas_cuda.so")
 CLI = os.path.join(BIN_DIR, "kgwas")
 CLI2 = os.path.join(BIN_DIR, "kgwas_2d")
+MERGE = os.path.join(BIN_DIR, "kgwas_index_merge")
 MMA_RATE = os.path.join(BIN_DIR, "mma_rate")
 OBJ_DIR = os.path.join(PKG, "_build")
 
@@ -30,6 +31,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIB_SOURCES = ["kernels.cu", "kernel_ts.cu", "kernel_mp.cu", "kernel_mpb.cu", "kernel_pairs.cu", "capi_pairs.cpp", "noalloc.cu", "capi.cpp", "capi_multi.cpp", "prep.cpp"]
 CLI_SOURCES = ["kgwas_main.cpp", "kgwas_io.cpp"]
 CLI2_SOURCES = ["kgwas2d_main.cpp", "kgwas_io.cpp"]
+MERGE_SOURCES = ["index_merge_main.cpp", "kgwas_io.cpp"]
 
 
 def nvcc() -> str:
@@ -113,6 +115,7 @@ def build_all(force=False, verbose=False):
     build_lib(force, verbose)
     build_cli(force, verbose)
     build_cli(force, verbose, CLI2, CLI2_SOURCES)
+    build_cli(force, verbose, MERGE, MERGE_SOURCES)
     build_mma_rate(force, verbose)
     return LIB, CLI
 

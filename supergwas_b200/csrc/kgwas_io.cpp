@@ -13,9 +13,11 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <filesystem>
 #include <fstream>
 #include <iostream>
 #include <memory>
+#include <sstream>
 
 #include <omp.h>
 
@@ -586,6 +588,197 @@ IndexBits load_index_bits(const std::string& dir, int threads) {
     out.bits[i] = std::move(all[i].second);
   }
   return out;
+}
+
+// ------------------------------------------------- sharded index (writer)
+
+bool canonical_kmer(const std::string& kmer, unsigned __int128& key) {
+  const size_t K = kmer.size();
+  if (K == 0 || K > 64) return false;
+  unsigned __int128 f = 0, r = 0;
+  for (size_t i = 0; i < K; ++i) {
+    int b;
+    switch (kmer[i]) {
+      case 'A': case 'a': b = 0; break;
+      case 'C': case 'c': b = 1; break;
+      case 'G': case 'g': b = 2; break;
+      case 'T': case 't': b = 3; break;
+      default: return false;
+    }
+    f = (f << 2) | (unsigned)b;
+    r |= (unsigned __int128)(3 - b) << (2 * i);  // complement, read backwards
+  }
+  key = f < r ? f : r;
+  return true;
+}
+
+namespace {
+
+uint64_t splitmix_final(uint64_t x) {  // finaliser of SplitMix64 (Steele, Lea, Flood 2014)
+  x ^= x >> 30;
+  x *= 0xbf58476d1ce4e5b9ULL;
+  x ^= x >> 27;
+  x *= 0x94d049bb133111ebULL;
+  x ^= x >> 31;
+  return x;
+}
+
+template <class T>
+void put(std::string& b, const T& v) {
+  b.append(reinterpret_cast<const char*>(&v), sizeof(T));
+}
+
+bool write_file(const std::string& path, const std::string& data) {
+  std::ofstream out(path, std::ios::binary);
+  if (!out) return false;
+  out.write(data.data(), (std::streamsize)data.size());
+  return (bool)out;
+}
+
+}  // namespace
+
+bool write_index(const std::string& dir, uint32_t K, uint32_t M, std::vector<IndexRow>& rows) {
+  std::error_code ec;
+  std::filesystem::create_directories(dir, ec);
+  std::vector<std::vector<IndexRow>> sh(M);
+  for (auto& r : rows) sh[(size_t)((uint64_t)r.key & (M - 1))].push_back(std::move(r));
+  static const char MAGIC[8] = {'U', 'M', 'A', 'P', 'd', '4', '\0', '\0'};
+  // shards are independent: sorted, deduplicated and written in parallel
+  auto write_shard = [&](uint32_t s) -> bool {
+    auto& v = sh[s];
+    std::stable_sort(v.begin(), v.end(), [](const IndexRow& a, const IndexRow& b) { return a.key < b.key; });
+    v.erase(std::unique(v.begin(), v.end(), [](const IndexRow& a, const IndexRow& b) { return a.key == b.key; }),
+            v.end());
+    char fname[32];
+    std::snprintf(fname, sizeof(fname), "shard_%03u", s);
+    const std::string stem = dir + "/" + fname;
+    std::string u;
+    u.append(MAGIC, 8);
+    put(u, K);
+    put(u, (uint64_t)v.size());
+    bool any_bits = false;
+    for (const auto& r : v) {
+      put(u, r.key);
+      put(u, r.effect);
+      put(u, r.pval);
+      any_bits = any_bits || !r.bits.empty();
+    }
+    if (!write_file(stem + ".umap", u)) {
+      std::cerr << "[ERROR] cannot write " << stem << ".umap\n";
+      return false;
+    }
+    if (any_bits) {
+      std::string b;
+      put(b, (uint64_t)v.size());
+      for (const auto& r : v) {
+        put(b, (uint32_t)r.bits.size());
+        b += r.bits;
+      }
+      if (!write_file(stem + ".bits", b)) {
+        std::cerr << "[ERROR] cannot write " << stem << ".bits\n";
+        return false;
+      }
+    }
+    // Bloom filter: m = 10 bits per entry rounded up to a power of two (64
+    // for an empty shard), two bit positions per key
+    uint64_t target = (uint64_t)v.size() * 10, m = 1;
+    if (target == 0) target = 64;
+    while (m < target) m <<= 1;
+    std::vector<uint64_t> words((m + 63) / 64, 0);
+    for (const auto& r : v) {
+      const uint64_t h1 = splitmix_final((uint64_t)r.key ^ (uint64_t)(r.key >> 64));
+      const uint64_t h2 = splitmix_final(h1);
+      const uint64_t i1 = h1 & (m - 1), i2 = h2 & (m - 1);
+      words[i1 >> 6] |= 1ull << (i1 & 63);
+      words[i2 >> 6] |= 1ull << (i2 & 63);
+    }
+    std::string bl;
+    put(bl, m);
+    put(bl, (uint64_t)words.size());
+    bl.append(reinterpret_cast<const char*>(words.data()), words.size() * 8);
+    if (!write_file(stem + ".bloom", bl)) {
+      std::cerr << "[ERROR] cannot write " << stem << ".bloom\n";
+      return false;
+    }
+    return true;
+  };
+  std::atomic<bool> ok{true};
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t s = 0; s < (int64_t)M; ++s)
+    if (!write_shard((uint32_t)s)) ok = false;
+  if (!ok) return false;
+  uint64_t total = 0;
+  for (const auto& v : sh) total += v.size();
+  std::ostringstream meta;
+  meta << "K=" << K << "\nM=" << M << "\nN=" << total << "\n";
+  if (!write_file(dir + "/index.meta", meta.str())) {
+    std::cerr << "[ERROR] cannot write index.meta in " << dir << "\n";
+    return false;
+  }
+  return true;
+}
+
+bool read_index_rows(const std::string& dir, uint32_t& K, uint32_t& M, std::vector<IndexRow>& rows) {
+  uint64_t N = 0;
+  if (!read_meta(dir, K, M, N)) return false;
+  static const char MAGIC[8] = {'U', 'M', 'A', 'P', 'd', '4', '\0', '\0'};
+  for (uint32_t s = 0; s < M; ++s) {
+    char fname[32];
+    std::snprintf(fname, sizeof(fname), "shard_%03u", s);
+    const std::string umap = dir + "/" + fname + ".umap", bitsp = dir + "/" + fname + ".bits";
+    std::vector<char> buf;
+    if (!slurp(umap, buf, "umap")) return false;
+    uint32_t k = 0;
+    uint64_t n = 0;
+    if (buf.size() < 20 || std::memcmp(buf.data(), MAGIC, 8) != 0) {
+      std::cerr << "[ERROR] bad magic in " << umap << "\n";
+      return false;
+    }
+    std::memcpy(&k, buf.data() + 8, 4);
+    std::memcpy(&n, buf.data() + 12, 8);
+    if (k != K) {
+      std::cerr << "[ERROR] K mismatch in " << umap << ": got " << k << " expected " << K << "\n";
+      return false;
+    }
+    if (buf.size() < 20 + (size_t)n * 32) {
+      std::cerr << "[ERROR] short read: " << umap << "\n";
+      return false;
+    }
+    const size_t r0 = rows.size();
+    rows.resize(r0 + (size_t)n);
+    for (uint64_t i = 0; i < n; ++i) {
+      IndexRow& r = rows[r0 + (size_t)i];
+      const char* p = buf.data() + 20 + i * 32;
+      std::memcpy(&r.key, p, 16);
+      std::memcpy(&r.effect, p + 16, 8);
+      std::memcpy(&r.pval, p + 24, 8);
+      r.k = K;
+    }
+    struct stat st;
+    if (stat(bitsp.c_str(), &st) != 0) continue;  // a shard without bitstrings has no .bits
+    std::vector<char> bb;
+    uint64_t bn = 0;
+    if (!slurp(bitsp, bb, "bits")) return false;
+    if (bb.size() >= 8) std::memcpy(&bn, bb.data(), 8);
+    if (bb.size() < 8 || bn != n) {
+      std::cerr << "[ERROR] .bits N=" << bn << " != .umap N=" << n << " in " << bitsp << "\n";
+      return false;
+    }
+    size_t off = 8;
+    for (uint64_t i = 0; i < n; ++i) {
+      uint32_t blen = 0;
+      if (off + 4 > bb.size()) return false;
+      std::memcpy(&blen, bb.data() + off, 4);
+      off += 4;
+      if (off + blen > bb.size()) {
+        std::cerr << "[ERROR] short read: " << bitsp << "\n";
+        return false;
+      }
+      rows[r0 + (size_t)i].bits.assign(bb.data() + off, blen);
+      off += blen;
+    }
+  }
+  return true;
 }
 
 }  // namespace kgio

@@ -84,4 +84,29 @@ struct IndexBits {
 };
 IndexBits load_index_bits(const std::string& dir, int threads);
 
+// Writing the same sharded index (the input of the 2-D test) straight from
+// emitted rows, without the text pass of the reference's build_index
+// (src/build_index.cpp:29-273): a k-mer is stored under its canonical 2-bit
+// encoding (the smaller of the k-mer and its reverse complement, A/C/G/T =
+// 0/1/2/3, first base most significant) in shard (encoding & (M - 1)); each
+// shard is sorted by encoding, duplicates keep one entry, and gets its .umap,
+// .bits (when any entry has a bitstring) and a 2-hash Bloom filter (.bloom,
+// 10 bits per entry rounded up to a power of two, SplitMix64 finaliser).
+struct IndexRow {
+  unsigned __int128 key = 0;  // canonical encoding
+  uint32_t k = 0;             // k-mer length
+  double effect = 0, pval = 0;
+  std::string bits;
+};
+// Canonical encoding of a k-mer; false if it holds a base other than ACGT/acgt
+// or is longer than 64.
+bool canonical_kmer(const std::string& kmer, unsigned __int128& key);
+// Writes index.meta and shard_%03u.{umap,bits,bloom}, s < M (M a power of 2);
+// returns false (with an [ERROR] line) when a file cannot be written.
+bool write_index(const std::string& dir, uint32_t K, uint32_t M, std::vector<IndexRow>& rows);
+// Appends every record of an index written as above, shard by shard in file
+// order, with its bitstring (empty where the shard has no .bits); sets K and M
+// from index.meta.  false (with an [ERROR] line) on a missing or malformed file.
+bool read_index_rows(const std::string& dir, uint32_t& K, uint32_t& M, std::vector<IndexRow>& rows);
+
 }  // namespace kgio

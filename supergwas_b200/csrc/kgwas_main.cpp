@@ -10,6 +10,12 @@
 // reference ignores:
 //   KGWAS_PRECISION  split (default: tcgen05 int8 limbs) | fp64 (CUDA cores)
 //   KGWAS_DEVICE     CUDA device ordinal (default 0)
+//   --index-out DIR     also write the .tsv rows as the sharded k-mer index
+//                       that the reference's build_index makes of the .tsv
+//                       file (--index-shards M, default 16)
+//   --index-2d-out DIR  the same for the .2d rows (the .2d.tsv file; 4 shards
+//                       by default, as build_index_2d.sh), the input of kgwas_2d
+//                       (bin/kgwas_index_merge joins the indexes of batches)
 //   KGWAS_KBITS      1: keep the packed rows of the batch in a sidecar file
 //                    <batch>/kgwas_<N>_<n>_<hash>.kbits (hash of the overlap
 //                    sample positions) and reuse it instead of re-reading the
@@ -46,6 +52,10 @@ struct Config {                      // src/kgwas.cpp:26-35
   string mode;
   int precision = KG_PREC_SPLIT_I8;
   int device = 0;
+  string index_out;     // --index-out DIR: the .tsv rows as a sharded index (build_index's output)
+  string index_2d_out;  // --index-2d-out DIR: the .2d rows as a sharded index
+  uint32_t index_shards = 16;    // build_index.sh's default
+  uint32_t index_2d_shards = 4;  // build_index_2d.sh's
 };
 
 static Config parse_args(int argc, char** argv) {  // src/kgwas.cpp:67-126
@@ -56,6 +66,9 @@ static Config parse_args(int argc, char** argv) {  // src/kgwas.cpp:67-126
               << "  INPUT: directory (batch with bits/ + kmers.txt.gz) for COLS mode,\n"
               << "         or a .tsv[.gz] file for ROWS mode.\n"
               << "  Auto-detects mode from INPUT type unless --mode is specified.\n"
+              << "\n"
+              << "  Index outputs: --index-out DIR [--index-shards M] (the .tsv rows),\n"
+              << "                 --index-2d-out DIR [--index-2d-shards M] (the .2d rows)\n"
               << "\n"
               << "  Env: LOAD_THREADS, BLAS_THREADS, EMIT_THREADS, CORR_THRESHOLD, BATCH_SIZE,\n"
               << "       KGWAS_PRECISION (split|fp64), KGWAS_DEVICE\n";
@@ -73,6 +86,14 @@ static Config parse_args(int argc, char** argv) {  // src/kgwas.cpp:67-126
       cfg.mode = argv[++i];
     } else if (a == "--log10-thresh-2d" && i + 1 < argc) {
       cfg.log10_thresh_2d = std::stod(argv[++i]);
+    } else if (a == "--index-out" && i + 1 < argc) {
+      cfg.index_out = argv[++i];
+    } else if (a == "--index-shards" && i + 1 < argc) {
+      cfg.index_shards = (uint32_t)std::stoul(argv[++i]);
+    } else if (a == "--index-2d-out" && i + 1 < argc) {
+      cfg.index_2d_out = argv[++i];
+    } else if (a == "--index-2d-shards" && i + 1 < argc) {
+      cfg.index_2d_shards = (uint32_t)std::stoul(argv[++i]);
     } else {
       try {
         cfg.log10_thresh = std::stod(a);
@@ -101,6 +122,12 @@ static Config parse_args(int argc, char** argv) {  // src/kgwas.cpp:67-126
     std::cerr << "[INFO] auto-detected mode: " << cfg.mode << "\n";
   }
   if (cfg.mode != "cols" && cfg.mode != "rows") die("--mode must be 'cols' or 'rows', got: " + cfg.mode);
+  auto pow2 = [](uint32_t m) { return m != 0 && (m & (m - 1)) == 0; };
+  if (!pow2(cfg.index_shards)) die("--index-shards must be a power of 2, got " + std::to_string(cfg.index_shards));
+  if (!pow2(cfg.index_2d_shards))
+    die("--index-2d-shards must be a power of 2, got " + std::to_string(cfg.index_2d_shards));
+  if (!cfg.index_2d_out.empty() && !(cfg.log10_thresh_2d > 0.0))
+    die("--index-2d-out needs the .2d rows (--log10-thresh-2d > 0)");
   return cfg;
 }
 
@@ -164,24 +191,73 @@ static void write_count(const string& out_file, uint64_t n_tested) {  // src/kgw
 }
 
 // Text of the emitted rows (src/kgwas.cpp:239-259): default ostream float
-// formatting (6 significant digits), k-mer order.
+// formatting (6 significant digits), k-mer order.  With index1/index2 the rows
+// are also kept for the index writer, with the values as printed (build_index
+// reads them back with strtod, src/build_index.cpp:89-90).
 static void format_hits(const kg_result& r, const vector<string>& kmers, const uint64_t* packed, uint32_t W,
-                        int n, bool do_2d, double p_thresh_2d, string& one, string& two) {
-  std::ostringstream o1, o2;
+                        int n, bool do_2d, double p_thresh_2d, string& one, string& two,
+                        vector<kgio::IndexRow>* index1 = nullptr, vector<kgio::IndexRow>* index2 = nullptr) {
+  std::ostringstream o1, o2, ev, pv;
   o1.setf(std::ios::fmtflags(0), std::ios::floatfield);
   o2.setf(std::ios::fmtflags(0), std::ios::floatfield);
   string bits(n, '0');
   for (uint64_t h = 0; h < r.n_hits; ++h) {
     const kg_hit& x = r.hits[h];
-    o1 << kmers[x.kmer] << '\t' << x.effect << '\t' << x.pval << '\n';
-    if (do_2d && x.pval <= p_thresh_2d) {
+    const string& km = kmers[x.kmer];
+    const bool is2 = do_2d && x.pval <= p_thresh_2d;
+    if (is2) {
       const uint64_t* row = packed + (size_t)x.kmer * W;
       for (int i = 0; i < n; ++i) bits[i] = ((row[i >> 6] >> (i & 63)) & 1u) ? '1' : '0';
-      o2 << kmers[x.kmer] << '\t' << bits << '\t' << x.effect << '\t' << x.pval << '\n';
     }
+    kgio::IndexRow ir;
+    if (!index1 && !(is2 && index2)) {
+      o1 << km << '\t' << x.effect << '\t' << x.pval << '\n';
+      if (is2) o2 << km << '\t' << bits << '\t' << x.effect << '\t' << x.pval << '\n';
+      continue;
+    }
+    // the values printed once (same stream formatting), then read back as
+    // build_index reads them
+    ev.str("");
+    pv.str("");
+    ev << x.effect;
+    pv << x.pval;
+    const string e = ev.str(), q = pv.str();
+    o1 << km << '\t' << e << '\t' << q << '\n';
+    if (is2) o2 << km << '\t' << bits << '\t' << e << '\t' << q << '\n';
+    if (!kgio::canonical_kmer(km, ir.key)) continue;  // a base other than ACGT: build_index skips the row
+    ir.effect = std::strtod(e.c_str(), nullptr);
+    ir.pval = std::strtod(q.c_str(), nullptr);
+    ir.k = (uint32_t)km.size();
+    if (is2 && index2) {
+      kgio::IndexRow r2 = ir;
+      r2.bits = bits;
+      index2->push_back(std::move(r2));
+    }
+    if (index1) index1->push_back(std::move(ir));
   }
   one = o1.str();
   two = o2.str();
+}
+
+// Writes one index (build_index on this run's .tsv or .2d.tsv file): k from
+// the first row, rows of another length left out (src/build_index.cpp:73-75,
+// 153-156).  Without rows, k is the first k-mer's length and every shard is
+// empty (build_index instead stops with "Could not infer k-mer length").
+static void write_index_out(const string& dir, uint32_t M, const char* what, const vector<string>& kmers,
+                            vector<kgio::IndexRow>& rows) {
+  if (dir.empty()) return;
+  const uint32_t K = !rows.empty() ? rows[0].k : kmers.empty() ? 0u : (uint32_t)kmers[0].size();
+  rows.erase(std::remove_if(rows.begin(), rows.end(), [K](const kgio::IndexRow& r) { return r.k != K; }),
+             rows.end());
+  const size_t n_rows = rows.size();
+  if (!kgio::write_index(dir, K, M, rows)) die("Failed to write index " + dir);
+  std::cerr << "[INFO] wrote " << n_rows << " " << what << " rows as a " << M << "-shard index to " << dir << "\n";
+}
+
+static void write_indexes(const Config& cfg, const vector<string>& kmers, vector<kgio::IndexRow>& rows1,
+                          vector<kgio::IndexRow>& rows2) {
+  write_index_out(cfg.index_out, cfg.index_shards, ".tsv", kmers, rows1);
+  write_index_out(cfg.index_2d_out, cfg.index_2d_shards, ".2d", kmers, rows2);
 }
 
 // ---------------------------------------------------------- .kbits cache
@@ -281,7 +357,9 @@ static void run_cols(const Config& cfg) {  // src/kgwas.cpp:168-307
   const bool do_2d = (cfg.log10_thresh_2d > 0.0);
   const double p_thresh_2d = do_2d ? std::pow(10.0, -cfg.log10_thresh_2d) : 0.0;
   string one, two;
-  format_hits(res, kmers, X.p, W, n, do_2d, p_thresh_2d, one, two);
+  vector<kgio::IndexRow> index1, index2;
+  format_hits(res, kmers, X.p, W, n, do_2d, p_thresh_2d, one, two, cfg.index_out.empty() ? nullptr : &index1,
+              cfg.index_2d_out.empty() ? nullptr : &index2);
   {
     std::ofstream out(cfg.out_file, std::ios::binary);
     if (!out) die("open out: " + cfg.out_file);
@@ -300,6 +378,7 @@ static void run_cols(const Config& cfg) {  // src/kgwas.cpp:168-307
     if (!out2d) die("write 2D out failed");
     std::cerr << "[INFO] wrote 2D hits at -log10(p) >= " << cfg.log10_thresh_2d << " to " << p2 << "\n";
   }
+  write_indexes(cfg, kmers, index1, index2);
   write_count(cfg.out_file, res.n_tested);
   std::cerr << "[TIME] total " << tall.sec() << " s\n";
 }
@@ -353,6 +432,8 @@ static void run_rows(const Config& cfg) {  // src/kgwas.cpp:343-522
   const size_t BATCH = (size_t)1 << 22;
   vector<string> kmers;
   vector<uint64_t> packed;
+  vector<kgio::IndexRow> index1, index2;
+  string first_kmer;
   for (;;) {
     kmers.clear();
     packed.clear();
@@ -362,7 +443,9 @@ static void run_rows(const Config& cfg) {  // src/kgwas.cpp:343-522
     g.check(kg_run_host(g.ctx, packed.data(), got, W, &res, nullptr), "run");
     passed += res.n_tested;
     string one, two;
-    format_hits(res, kmers, packed.data(), W, n, do_2d, p_thresh_2d, one, two);
+    format_hits(res, kmers, packed.data(), W, n, do_2d, p_thresh_2d, one, two,
+                cfg.index_out.empty() ? nullptr : &index1, cfg.index_2d_out.empty() ? nullptr : &index2);
+    if (first_kmer.empty() && !kmers.empty()) first_kmer = kmers[0];
     out.write(one.data(), (std::streamsize)one.size());
     if (do_2d) out2d.write(two.data(), (std::streamsize)two.size());
   }
@@ -372,6 +455,7 @@ static void run_rows(const Config& cfg) {  // src/kgwas.cpp:343-522
     std::cerr << "[INFO] 2D hits written to " << p2 << "\n";
   }
   out.close();
+  write_indexes(cfg, vector<string>{first_kmer}, index1, index2);
   write_count(cfg.out_file, passed);
   std::cerr << "[TIME] End-to-end " << tall.sec() << "s\n";
 }

@@ -523,6 +523,27 @@ def make_pair_faults():
     return out
 
 
+def make_index():
+    """The reference build_index on the small fixture's reference kgwas
+    outputs (all rows): the .2d.tsv at 4 shards and the .tsv at the default 16,
+    the sharded indexes that kgwas --index-2d-out / --index-out must reproduce
+    byte for byte (src/build_index.cpp)."""
+    d = os.path.join(HERE, "index")
+    os.makedirs(d, exist_ok=True)
+    shutil.copy(os.path.join(HERE, "small", "ref_cols_all.2d.tsv"), os.path.join(d, "input.2d.tsv"))
+    out = os.path.join(d, "ref_index")
+    if os.path.isdir(out):
+        shutil.rmtree(out)
+    r = O.run_reference_tool("build_index", [os.path.join(d, "input.2d.tsv"), out, "--shards", "4"])
+    assert r.returncode == 0, r.stderr
+    # the 1-D index of the 3-column .tsv rows, at build_index's default 16 shards
+    out = os.path.join(d, "ref_index_1d")
+    if os.path.isdir(out):
+        shutil.rmtree(out)
+    r = O.run_reference_tool("build_index", [os.path.join(HERE, "small", "ref_cols_all.tsv"), out])
+    assert r.returncode == 0, r.stderr
+
+
 def make_pairs():
     """2-D pair test (src/kgwas_2d.cpp): a kgwas-style .2d.tsv of k-mers with
     bitstrings is turned into a sharded index by the reference's build_index
@@ -603,7 +624,7 @@ def make_pairs():
 if __name__ == "__main__":
     if not O.ref_available():
         sys.exit("stage the reference first: bash oracle/stage_ref.sh")
-    names = sys.argv[1:] or [*FIXTURES, "cfg1", "faults", "pairs", "pair_faults"]
+    names = sys.argv[1:] or [*FIXTURES, "cfg1", "faults", "pairs", "pair_faults", "index"]
     for nm in names:
         if nm == "cfg1":
             make_cfg1()
@@ -611,6 +632,8 @@ if __name__ == "__main__":
             make_pairs()
         elif nm == "pair_faults":
             make_pair_faults()
+        elif nm == "index":
+            make_index()
         elif nm == "faults":
             make_faults()
         else:

@@ -121,3 +121,26 @@ def compare_rows(got_rows, ref_rows, kmers, band, rel_tol, abs_floor=1e-300):
         for x, y in zip(map(float, a[-2:]), map(float, b[-2:])):
             assert abs(x - y) <= rel_tol * max(abs(y), abs(x)) + abs_floor, (a, b)
     return len(g)
+
+
+def index_check_lib():
+    """tests/native/index_check.cpp with the library's index writer
+    (supergwas_b200/csrc/kgwas_io.cpp), built with g++ on first use:
+    ``index_from_tsv(tsv, dir, M)`` writes the sharded index of a .tsv or .2d.tsv."""
+    import ctypes
+    here = os.path.dirname(os.path.abspath(__file__))
+    out = os.path.join(here, "native", "_build", "libindex_check.so")
+    src = [os.path.join(here, "native", "index_check.cpp"), os.path.join(build.CSRC, "kgwas_io.cpp")]
+    if not os.path.exists(out) or any(os.path.getmtime(s) > os.path.getmtime(out) for s in src):
+        os.makedirs(os.path.dirname(out), exist_ok=True)
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", out, *src, "-lz"],
+                       check=True)
+    return ctypes.CDLL(out)
+
+
+def same_dir_files(a, b):
+    """Both directories hold the same file names with byte-identical contents."""
+    assert sorted(os.listdir(a)) == sorted(os.listdir(b))
+    for f in os.listdir(b):
+        assert open(os.path.join(a, f), "rb").read() == open(os.path.join(b, f), "rb").read(), f
+

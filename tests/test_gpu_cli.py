@@ -102,3 +102,39 @@ def test_kbits_sidecar_reuse(built):
         outs.append((open(out).read(), open(out + ".count").read()))
     assert outs[0] == outs[1]
     shutil.rmtree(work)
+
+
+def _build_index_like(tsv, out, shards):
+    """The index that build_index makes of one kgwas output file: the staged
+    reference build_index when present, else the library's writer (pinned to
+    build_index's own files by the CPU suite)."""
+    if os.access(os.path.join(O.REF_DIR, "build_index"), os.X_OK):
+        r = O.run_reference_tool("build_index", [tsv, out, "--shards", str(shards)])
+        assert r.returncode == 0, r.stderr[-2000:]
+    else:
+        assert H.index_check_lib().index_from_tsv(tsv.encode(), out.encode(), shards) == 0
+
+
+@pytest.mark.parametrize("mode", ["cols", "rows"])
+def test_index_out_matches_build_index(built, mode):
+    """--index-out / --index-2d-out write the .tsv and .2d rows as sharded
+    k-mer indexes: the same files (index.meta, shard_*.umap/.bits/.bloom) that
+    the reference build_index writes from the .tsv and the .2d.tsv
+    (src/build_index.cpp), here on GPU-emitted rows."""
+    import shutil
+    work = tempfile.mkdtemp()
+    paths, rows = H.materialise("small", work)
+    out = os.path.join(work, "run", "batch_000.tsv")
+    os.makedirs(os.path.dirname(out))
+    idx1, idx2 = os.path.join(work, "idx1"), os.path.join(work, "idx2")
+    inp = paths["batch"] if mode == "cols" else rows
+    r = H.run_cli([paths["samples"], paths["pheno"], inp, paths["ubin"], out, "0", "--log10-thresh-2d", "1",
+                   "--mode", mode, "--index-out", idx1, "--index-2d-out", idx2])
+    assert r.returncode == 0, r.stderr[-2000:]
+    two = O.path_2d(out)
+    assert len(H.parse_rows(out)) > 1000 and len(H.parse_rows(two)) > 100
+    _build_index_like(out, os.path.join(work, "ref1"), 16)
+    _build_index_like(two, os.path.join(work, "ref2"), 4)
+    H.same_dir_files(idx1, os.path.join(work, "ref1"))
+    H.same_dir_files(idx2, os.path.join(work, "ref2"))
+    shutil.rmtree(work)

@@ -214,3 +214,56 @@ def test_kgwas_2d_errors_match_reference(built):
         finally:
             shutil.rmtree(work)
 
+
+def test_index_writer_matches_build_index(tmp_path):
+    """The index writer of kgwas --index-out / --index-2d-out (kgio::write_index)
+    on the rows of a reference .2d.tsv and .tsv gives the files of the
+    reference build_index byte for byte:
+    index.meta, and per shard the .umap, .bits and .bloom (src/build_index.cpp,
+    src/map_utils.hpp:109-160, 331-372, 562-575)."""
+    L = H.index_check_lib()
+    d = os.path.join(H.GOLDEN, "index")
+    got = str(tmp_path / "idx")
+    assert L.index_from_tsv(os.path.join(d, "input.2d.tsv").encode(), got.encode(), 4) == 0
+    H.same_dir_files(got, os.path.join(d, "ref_index"))
+    # the 1-D index of the 3-column .tsv rows: 16 shards, no .bits files
+    got = str(tmp_path / "idx1")
+    tsv = os.path.join(H.GOLDEN, "small", "ref_cols_all.tsv")
+    assert L.index_from_tsv(tsv.encode(), got.encode(), 16) == 0
+    H.same_dir_files(got, os.path.join(d, "ref_index_1d"))
+
+
+def test_index_merge_matches_build_index(built, tmp_path):
+    """bin/kgwas_index_merge joins per-batch indexes into the index that
+    build_index makes of all the batches' rows: the golden .2d.tsv split into
+    three batches, each indexed on its own (2 shards), merged to 4 shards, gives
+    the reference build_index's files of the whole .2d.tsv byte for byte."""
+    d = os.path.join(H.GOLDEN, "index")
+    lines = open(os.path.join(d, "input.2d.tsv")).read().splitlines(keepends=True)
+    L = H.index_check_lib()
+    parts = []
+    for b, chunk in enumerate((lines[:100], lines[100:101], lines[101:])):
+        tsv = tmp_path / f"batch_{b:03d}.2d.tsv"
+        tsv.write_text("".join(chunk))
+        out = str(tmp_path / f"idx_{b}")
+        assert L.index_from_tsv(str(tsv).encode(), out.encode(), 2) == 0
+        parts.append(out)
+    merged = str(tmp_path / "merged")
+    r = subprocess.run([build.MERGE, merged, *parts, "--shards", "4"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    H.same_dir_files(merged, os.path.join(d, "ref_index"))
+    # a K mismatch or a missing input is an [ERROR] exit
+    r = subprocess.run([build.MERGE, str(tmp_path / "bad"), parts[0], str(tmp_path / "none")],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "[ERROR]" in r.stderr
+
+
+def test_index_out_option_errors(built, tmp_path):
+    """The index options are checked before any input or GPU is touched."""
+    base = ["s.txt", "p.txt", "in", "U.bin", str(tmp_path / "o.tsv"), "--mode", "cols"]
+    for extra, msg in ((["--index-2d-out", "d", "--log10-thresh-2d", "0"], "--index-2d-out needs the .2d rows"),
+                       (["--index-out", "d", "--index-shards", "12"], "--index-shards must be a power of 2"),
+                       (["--index-2d-shards", "0"], "--index-2d-shards must be a power of 2")):
+        r = H.run_cli([*base, *extra])
+        assert r.returncode == 1 and msg in r.stderr, (extra, r.stderr)
+
