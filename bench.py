@@ -537,6 +537,86 @@ def run_streaming(args):
     api.lib().kg_host_free(hbuf)
 
 
+SORTED = dict(n=1000, m=50_000_000, S=8, r=16, n_causal=50, missing=0.05, seed=49, mean_run=5)
+
+
+def run_sorted(args):
+    """End to end (kg_run_host from pinned host memory) on a batch sorted by
+    bit pattern, as real batches are (src/convert_matrix.cpp:366-368): each
+    distinct row repeated 1..9 times (mean 5).  One row per run is copied and
+    tested; timed against the same call testing every row (KG_DEDUP=0)."""
+    import ctypes
+    import torch
+    from supergwas_b200 import api, build, synth_gpu
+    rank, world, local = rank_env()
+    torch.cuda.set_device(local)
+    build.build_all()
+    W = dict(SORTED)
+    if args.kmers:
+        W["m"] = args.kmers
+    n, m, r, mr = W["n"], W["m"], W["r"], W["mean_run"]
+    wpk = (n + 63) // 64
+    wpk += wpk & 1
+    t_gen = time.perf_counter()
+    gen = torch.Generator(device="cuda").manual_seed(W["seed"] + 1000 * rank)
+    reps = torch.randint(1, 2 * mr, (int(1.2 * m / mr) + 64,), device="cuda", generator=gen)
+    cum = reps.cumsum(0)
+    d = int((cum < m).sum()) + 1
+    reps = reps[:d].clone()
+    reps[-1] -= int(cum[d - 1]) - m
+    Xd = synth_gpu.gen_packed(n, d, W["S"], W["seed"] + 1000 * rank)
+    U, y, keep, _ = synth_gpu.structure_and_phenotype(Xd, n, r, W["n_causal"], W["missing"], W["seed"] + 1000 * rank)
+    nbytes = m * wpk * 8
+    hbuf = api.lib().kg_host_alloc(nbytes)
+    if not hbuf:
+        raise RuntimeError("kg_host_alloc failed")
+    ht = torch.frombuffer((ctypes.c_char * nbytes).from_address(hbuf), dtype=torch.int64).view(m, wpk)
+    ht.copy_(torch.repeat_interleave(Xd, reps, dim=0))
+    del Xd
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t_gen
+    g = api.Kgwas(device=local, precision="split", corr_threshold=0.0, log10_thresh=6.0)
+    g.set_structure(U, y, keep, n)
+
+    def timed(steps):
+        for _ in range(args.warmup):
+            g.run_host_ptr(hbuf, m, wpk)
+        t0 = time.perf_counter()
+        tests = 0
+        for _ in range(steps):
+            res = g.run_host_ptr(hbuf, m, wpk)
+            tests += res.n_tested
+        return tests, time.perf_counter() - t0, res
+
+    with Clocks(local) as ck:
+        tests, t, res = timed(args.steps)
+    unique = g.last_unique_rows()
+    launches = g.last_launch_count()
+    os.environ["KG_DEDUP"] = "0"
+    steps0 = max(1, min(args.steps, 3))
+    tests0, t0, res0 = timed(steps0)
+    del os.environ["KG_DEDUP"]
+    assert res0.n_tested == res.n_tested and res0.hits.shape[0] == res.hits.shape[0]
+    value = tests / t
+    line = {"metric": "k-mer tests/s end to end (kg_run_host, pinned host) on a batch sorted by bit pattern",
+            "value": value, "unit": "k-mer tests/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "i8 limbs -> i32 TMEM, f64 epilogue", "data": "synthetic (seeded, generated on device)",
+            "config": {"workload": f"sorted: n={n} (5% unphenotyped), {m} k-mers per step from {d} distinct rows "
+                                   f"(runs of 1..9, mean {mr}), r={r}+1, 1 phenotype, CORR_THRESHOLD=0",
+                       "parallelism": f"weak: {world} GPU(s)"},
+            "e2e": {"value": value, "unit": "k-mer tests/s", "h2d_bytes_per_step": unique * wpk * 8 + unique * 4,
+                    "d2h_bytes_per_step": 3 * 8 + int(res.hits.shape[0]) * 32},
+            "rows_tested_per_step": unique, "every_row": {"value": tests0 / t0, "unit": "k-mer tests/s",
+                                                          "h2d_bytes_per_step": nbytes},
+            "speedup_vs_every_row": value / (tests0 / t0),
+            "gpu_launches": launches, "clocks": ck.summary(), "gen_seconds": t_gen}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    g.close()
+    api.lib().kg_host_free(hbuf)
+
+
 PAIRS = dict(n=1000, N=50_000, S=8, r=16, seed=48, cpu_N=3000)
 
 
@@ -645,9 +725,11 @@ def main():
     ap.add_argument("--cpu-kmers", type=int, default=1_000_000)
     ap.add_argument("--ref-kmers", type=int, default=250_000)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="precision", choices=["precision", "batched", "streaming", "pairs"],
+    ap.add_argument("--workload", default="precision",
+                    choices=["precision", "batched", "streaming", "pairs", "sorted"],
                     help="precision: the default single-phenotype workload; batched: 64 phenotypes; "
-                         "streaming: 8 phenotypes at n=5000 from pinned host memory; pairs: the 2-D pair test")
+                         "streaming: 8 phenotypes at n=5000 from pinned host memory; pairs: the 2-D pair test; "
+                         "sorted: end to end on a batch with runs of equal rows")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours" and not os.environ.get("KG_BENCH_ALLOW_SHORT"):
         args.warmup = 3
@@ -659,6 +741,8 @@ def main():
         run_streaming(args)
     elif args.workload == "pairs":
         run_pairs(args)
+    elif args.workload == "sorted":
+        run_sorted(args)
     else:
         run_ours(args)
 

@@ -232,6 +232,15 @@ int kg_last_launch_count(const kg_ctx* ctx);
  * memory; shapes the first does not cover) or "fp64" (CUDA cores). */
 const char* kg_last_kernel(const kg_ctx* ctx);
 
+/* Rows the last kg_run_host tested on the device when it used runs of equal
+ * adjacent rows (0 when it tested every row).  Batches sorted by bit pattern
+ * (src/convert_matrix.cpp:366-368) hold such runs; one row per run is tested,
+ * counts once per row of its run in n_tested, and its hit is repeated for
+ * every row of the run, so the result is the same as without runs.  Not used
+ * when kg_stats outputs are requested; KG_DEDUP=0 in the environment turns
+ * it off. */
+uint64_t kg_last_unique_rows(const kg_ctx* ctx);
+
 const char* kg_last_error(const kg_ctx* ctx);
 void kg_destroy(kg_ctx* ctx);
 

@@ -112,6 +112,8 @@ def lib():
     L.kg_last_launch_count.argtypes = [vp]
     L.kg_last_kernel.argtypes = [vp]
     L.kg_last_kernel.restype = ctypes.c_char_p
+    L.kg_last_unique_rows.argtypes = [vp]
+    L.kg_last_unique_rows.restype = ctypes.c_uint64
     L.kg_last_error.argtypes = [vp]
     L.kg_last_error.restype = ctypes.c_char_p
     L.kg_destroy.argtypes = [vp]
@@ -332,6 +334,10 @@ class Kgwas:
 
     def last_kernel(self) -> str:
         return self._L.kg_last_kernel(self._h).decode()
+
+    def last_unique_rows(self) -> int:
+        """Rows the last run_host tested when it used runs of equal adjacent rows (0: every row)."""
+        return int(self._L.kg_last_unique_rows(self._h))
 
 
 def run_device_noalloc(d_x: int, m: int, wpk: int, U, y, corr_threshold: float, log10_thresh: float,

@@ -96,6 +96,7 @@ void kg_destroy(kg_ctx* ctx) {
   dfree(ctx->dPX);
   dfree(ctx->dPairs);
   dfree(ctx->dUnitOff);
+  dfree(ctx->dWeight);
   for (auto& p : ctx->dStat) dfree(p);
   for (int b = 0; b < NBUF; ++b) {
     dfree(ctx->dChunk[b]);
@@ -268,6 +269,7 @@ int launch_one(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, uint64
   O.kmer_offset = offset;
   O.cand = ctx->dCand;
   O.cand_cap = ctx->cand_cap;
+  O.weight = ctx->cur_weight;
   if (stats) {
     O.tested = ctx->dTested;
     O.chisq = ctx->dStat[0];
@@ -361,7 +363,77 @@ void par_memcpy(void* dst, const void* src, size_t bytes) {
   for (auto& t : th) t.join();
 }
 
-int run_host_once(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t wpk, bool stats) {
+// Gathers rows sel[0..cnt) of x into dst (row bytes each), in parallel for
+// large copies.
+void par_gather(void* dst, const uint64_t* x, const uint64_t* sel, uint64_t cnt, size_t row) {
+  auto body = [=](uint64_t a, uint64_t b) {
+    for (uint64_t u = a; u < b; ++u) std::memcpy((char*)dst + u * row, (const char*)x + sel[u] * row, row);
+  };
+  const size_t kMin = (size_t)64 << 20;
+  unsigned nt = std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
+  if (cnt * row < kMin || nt == 1) {
+    body(0, cnt);
+    return;
+  }
+  std::vector<std::thread> th;
+  const uint64_t per = (cnt + nt - 1) / nt;
+  for (unsigned t = 0; t < nt; ++t) {
+    const uint64_t a = t * per, b = std::min<uint64_t>(cnt, a + per);
+    if (a >= b) break;
+    th.emplace_back(body, a, b);
+  }
+  for (auto& t : th) t.join();
+}
+
+// Runs of equal adjacent rows.  Real batches are sorted by bit pattern
+// (src/convert_matrix.cpp:366-368), so equal rows sit next to each other; an
+// equal row has equal statistics, so one row per run is tested and counts as
+// many tested k-mers as the run has rows.  4096 sampled adjacent pairs decide
+// whether the full scan can pay (at least 10 % repeats); the runs are used
+// when they save at least 10 % of the rows.  KG_DEDUP=0 switches this off,
+// KG_DEDUP=1 uses the runs whenever any row repeats.
+bool find_runs(kg_ctx* ctx, const uint64_t* x, uint64_t m, uint32_t wpk) {
+  const char* v = std::getenv("KG_DEDUP");
+  const bool off = v && std::string(v) == "0", force = v && std::string(v) == "1";
+  if (off || m < 2 || m >= (1ull << 32)) return false;
+  const size_t row = (size_t)wpk * 8;
+  auto same = [&](uint64_t i) { return std::memcmp(x + i * wpk, x + (i - 1) * wpk, row) == 0; };
+  if (!force) {
+    if (m < 4096) return false;
+    int dups = 0;
+    for (int i = 0; i < 4096; ++i) dups += same(1 + (uint64_t)i * (m - 1) / 4096) ? 1 : 0;
+    if (dups * 10 < 4096) return false;
+  }
+  unsigned nt = std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency()));
+  if (m < (1u << 16)) nt = 1;
+  std::vector<std::vector<uint64_t>> starts(nt);
+  auto scan = [&](unsigned t) {
+    const uint64_t a = m * t / nt, b = m * (t + 1) / nt;
+    for (uint64_t i = a; i < b; ++i)
+      if (i == 0 || !same(i)) starts[t].push_back(i);
+  };
+  if (nt == 1) {
+    scan(0);
+  } else {
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t) th.emplace_back(scan, t);
+    for (auto& t : th) t.join();
+  }
+  size_t nu = 0;
+  for (auto& s : starts) nu += s.size();
+  if (force ? nu == m : nu * 10 > m * 9) return false;
+  ctx->run_first.clear();
+  ctx->run_first.reserve(nu);
+  for (auto& s : starts) ctx->run_first.insert(ctx->run_first.end(), s.begin(), s.end());
+  ctx->run_len.resize(nu);
+  for (size_t u = 0; u < nu; ++u)
+    ctx->run_len[u] = (uint32_t)((u + 1 < nu ? ctx->run_first[u + 1] : m) - ctx->run_first[u]);
+  return true;
+}
+
+// sel (optional): test rows sel[0..m) of xbits, gathered on the host.
+int run_host_once(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t wpk, bool stats,
+                  const uint64_t* sel = nullptr) {
   const size_t row = (size_t)wpk * 8;
   size_t want = (size_t)512 << 20;
   if (const char* v = std::getenv("KG_CHUNK_MB")) want = (size_t)std::max(1, std::atoi(v)) << 20;
@@ -369,7 +441,7 @@ int run_host_once(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t wpk, 
   if (per > m) per = m;
   const size_t bytes = (size_t)per * row;
   cudaPointerAttributes attr{};
-  bool pinned = cudaPointerGetAttributes(&attr, xbits) == cudaSuccess &&
+  bool pinned = !sel && cudaPointerGetAttributes(&attr, xbits) == cudaSuccess &&
                 (attr.type == cudaMemoryTypeHost || attr.type == cudaMemoryTypeManaged);
   cudaGetLastError();
   if (ctx->chunk_bytes < bytes) {
@@ -397,7 +469,10 @@ int run_host_once(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t wpk, 
       KG_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_k[b], 0), "wait");
       if (!pinned) KG_CUDA(cudaEventSynchronize(ctx->ev_h2d[b]), "sync");
     }
-    if (!pinned) {
+    if (sel) {
+      par_gather(ctx->hStage[b], xbits, sel + s, cnt, row);
+      src = (const char*)ctx->hStage[b];
+    } else if (!pinned) {
       par_memcpy(ctx->hStage[b], src, nb);
       src = (const char*)ctx->hStage[b];
     }
@@ -426,21 +501,65 @@ int kg_run_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t wpk, kg
   if (rc) return rc;
   ctx->pending = false;
   ctx->launches = 0;
+  ctx->unique_rows = 0;
   const bool stats = want_stats(st);
   if (stats && (rc = ensure_stats(ctx, m))) return rc;
   if ((rc = ensure_hits(ctx, std::max<unsigned long long>(ctx->hit_cap, 1ull << 16)))) return rc;
   if ((rc = ensure_cand(ctx, std::max<unsigned long long>(ctx->cand_cap, 1ull << 20)))) return rc;
   std::memset(ctx->counters, 0, sizeof(ctx->counters));
-  if (m) {
-    if ((rc = run_host_once(ctx, xbits, m, wpk, stats))) return rc;
+  // per-k-mer outputs are kept for every row, so runs are only used without them
+  const bool dedup = !stats && find_runs(ctx, xbits, m, wpk);
+  const uint64_t* sel = nullptr;
+  uint64_t mt = m;  // rows tested on the device
+  if (dedup) {
+    mt = ctx->run_first.size();
+    sel = ctx->run_first.data();
+    if (ctx->weight_cap < mt) {
+      dfree(ctx->dWeight);
+      ctx->weight_cap = 0;
+      KG_CUDA(cudaMalloc((void**)&ctx->dWeight, mt * sizeof(uint32_t)), "cudaMalloc(run lengths)");
+      ctx->weight_cap = mt;
+    }
+    KG_CUDA(cudaMemcpyAsync(ctx->dWeight, ctx->run_len.data(), mt * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                            ctx->stream),
+            "copy run lengths");
+    ctx->cur_weight = ctx->dWeight;
+    ctx->unique_rows = mt;
+  }
+  struct Reset {
+    kg_ctx* c;
+    ~Reset() { c->cur_weight = nullptr; }
+  } reset{ctx};
+  if (mt) {
+    if ((rc = run_host_once(ctx, xbits, mt, wpk, stats, sel))) return rc;
     for (int retry = 0; retry < 8 && (ctx->counters[2] & (kg::ERR_HIT_OVERFLOW | kg::ERR_CAND_OVERFLOW)); ++retry) {
       if ((ctx->counters[2] & kg::ERR_HIT_OVERFLOW) && (rc = ensure_hits(ctx, ctx->counters[1]))) return rc;
       if ((ctx->counters[2] & kg::ERR_CAND_OVERFLOW) && (rc = ensure_cand(ctx, 4 * ctx->cand_cap))) return rc;
-      if ((rc = run_host_once(ctx, xbits, m, wpk, stats))) return rc;
+      if ((rc = run_host_once(ctx, xbits, mt, wpk, stats, sel))) return rc;
     }
   }
-  return collect(ctx, m, res, st, stats);
+  if ((rc = collect(ctx, mt, res, st, stats))) return rc;
+  if (dedup) {
+    // every row of a run gets its run's row, in row order
+    std::vector<kg_hit> all;
+    for (const kg_hit& h : ctx->hits) {
+      const uint64_t f = ctx->run_first[h.kmer], e = f + ctx->run_len[h.kmer];
+      for (uint64_t i = f; i < e; ++i) {
+        all.push_back(h);
+        all.back().kmer = i;
+      }
+    }
+    ctx->hits.swap(all);
+    if (res) {
+      res->n_kmers = m;
+      res->n_hits = ctx->hits.size();
+      res->hits = ctx->hits.data();
+    }
+  }
+  return KG_OK;
 }
+
+uint64_t kg_last_unique_rows(const kg_ctx* ctx) { return ctx ? ctx->unique_rows : 0; }
 
 int kg_launch_device(kg_ctx* ctx, const uint64_t* d_x, uint64_t m, uint32_t wpk, void* stream) {
   if (!ctx) return KG_ERR_INVALID;

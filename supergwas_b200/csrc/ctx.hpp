@@ -147,6 +147,14 @@ struct kg_ctx {
   void* hStage[kgctx::NBUF] = {};
   size_t chunk_bytes = 0;
   cudaEvent_t ev_h2d[kgctx::NBUF] = {}, ev_k[kgctx::NBUF] = {};
+  // runs of equal adjacent rows (kg_run_host): first row and length of each
+  // run; the device copy of the lengths weighs the tested count
+  std::vector<uint64_t> run_first;
+  std::vector<uint32_t> run_len;
+  uint32_t* dWeight = nullptr;
+  size_t weight_cap = 0;
+  const uint32_t* cur_weight = nullptr;  // set while a deduplicated run is in flight
+  uint64_t unique_rows = 0;              // rows the last kg_run_host tested (0: no deduplication)
   // many phenotypes
   kgctx::Multi mp;
   // 2-D pair test

@@ -322,8 +322,13 @@ __device__ __forceinline__ void emit_kmer(const DevOut& O, unsigned long long lo
                                           bool hit, bool cand, double T, double p, double effect, double xxM,
                                           double xyM, double cor) {
   const unsigned lane = threadIdx.x & 31u;
-  const unsigned tmask = __ballot_sync(0xffffffffu, tested);
-  if (lane == 0 && tmask) atomicAdd(O.counters + 0, (unsigned long long)__popc(tmask));
+  if (O.weight) {
+    const unsigned tot = __reduce_add_sync(0xffffffffu, tested ? O.weight[O.kmer_offset + local] : 0u);
+    if (lane == 0 && tot) atomicAdd(O.counters + 0, (unsigned long long)tot);
+  } else {
+    const unsigned tmask = __ballot_sync(0xffffffffu, tested);
+    if (lane == 0 && tmask) atomicAdd(O.counters + 0, (unsigned long long)__popc(tmask));
+  }
   emit_rare(O, local, hit, cand, T, p, effect);
   if (valid && O.tested) {
     const unsigned long long g = O.kmer_offset + local;
@@ -432,7 +437,7 @@ __device__ __forceinline__ void finish_kmer_lean(const EpiParams& P, const DevOu
     const double xyc = ey + gs + P.kappa * cd;
     tested = tested && xyc * xyc >= P.thr2_ynorm2 * xcn2;
   }
-  tested_local += tested ? 1u : 0u;
+  if (tested) tested_local += O.weight ? O.weight[O.kmer_offset + local] : 1u;
   const double eps = 1e-12;
   const double xxM = cd - ss;
   const double xyM = P.b * cd + ey;

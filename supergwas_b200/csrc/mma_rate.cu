@@ -1,6 +1,6 @@
 // mma_rate.cu -- measurement program (bin/mma_rate): the rate of back-to-back
-// tcgen05.mma kind::i8 instructions per SM for M = 128 and several N, with A
-// from tensor memory or shared memory.  One CTA per SM; thread 0 issues 4096
+// tcgen05.mma kind::i8 instructions per SM for M = 128 or 64 and several N,
+// with A from tensor memory (M = 128) or shared memory.  One CTA per SM; thread 0 issues 4096
 // MMAs, commits them to an mbarrier, waits (bounded, 2 s) and records the
 // cycles.  It sets the ceiling of the association kernels: an instruction
 // costs max(~62 cycles, N / 2 cycles), so N = 64 reaches half the int8 peak.
@@ -10,8 +10,9 @@
 #include "device.cuh"
 using namespace kg;
 
-template <int N, bool ASMEM, int NACC>
+template <int M, int N, bool ASMEM, int NACC>
 __global__ void __launch_bounds__(128, 1) mma_bench(int iters, unsigned long long* out) {
+  static_assert(M == 128 || ASMEM, "A from tensor memory is measured at M = 128 only");
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -31,10 +32,10 @@ __global__ void __launch_bounds__(128, 1) mma_bench(int iters, unsigned long lon
   tc_fence_after();
   const uint32_t tmem = s_tmem;
   if (tid == 0) {
-    constexpr uint32_t IDESC = idesc_i8(128, N);
+    constexpr uint32_t IDESC = idesc_i8(M, N);
     const uint64_t bdesc0 = sdesc_noswz(sB, N * 16, 128);
-    const uint64_t adesc0 = sdesc_noswz(sA, 128 * 16, 128);
-    constexpr uint32_t BSTEP = (2 * N * 16) >> 4, ASTEP = (2 * 128 * 16) >> 4;
+    const uint64_t adesc0 = sdesc_noswz(sA, M * 16, 128);
+    constexpr uint32_t BSTEP = (2 * N * 16) >> 4, ASTEP = (2 * M * 16) >> 4;
     const unsigned long long t0 = clock64();
     for (int it = 0; it < iters; ++it) {
       const int st = it & 7;
@@ -57,15 +58,15 @@ __global__ void __launch_bounds__(128, 1) mma_bench(int iters, unsigned long lon
   if (tid < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
 }
 
-template <int N, bool ASMEM, int NACC>
+template <int M, int N, bool ASMEM, int NACC>
 void run(const char* name) {
   int iters = 4096;
   unsigned long long* d;
   cudaMalloc(&d, 148 * 3 * 8);
   const int need = N * 32 * 8 + 4096 * 8 + 8 + 1024;
   const int smem = need > 120 * 1024 ? need : 120 * 1024;  // one CTA per SM
-  cudaFuncSetAttribute(mma_bench<N, ASMEM, NACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  for (int rep = 0; rep < 3; ++rep) mma_bench<N, ASMEM, NACC><<<148, 128, smem>>>(iters, d);
+  cudaFuncSetAttribute(mma_bench<M, N, ASMEM, NACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  for (int rep = 0; rep < 3; ++rep) mma_bench<M, N, ASMEM, NACC><<<148, 128, smem>>>(iters, d);
   cudaError_t e = cudaDeviceSynchronize();
   unsigned long long h[148 * 3];
   cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
@@ -74,21 +75,24 @@ void run(const char* name) {
   for (int b = 0; b < 148; ++b) { issue += h[3 * b]; total += h[3 * b + 1]; err |= h[3 * b + 2]; }
   issue /= 148.0 * iters;
   total /= 148.0 * iters;
-  const double macs = 128.0 * N * 32;
-  printf("%-22s N=%3d  issue %.1f cyc/MMA  complete %.1f cyc/MMA  %.0f MAC/cyc/SM (%.1f%% of 8192)  %s err=%llu\n", name, N,
+  const double macs = (double)M * N * 32;
+  printf("%-22s M=%3d N=%3d  issue %.1f cyc/MMA  complete %.1f cyc/MMA  %.0f MAC/cyc/SM (%.1f%% of 8192)  %s err=%llu\n", name, M, N,
          issue, total, macs / total, 100.0 * macs / total / 8192.0, cudaGetErrorString(e), err);
   cudaFree(d);
 }
 
 int main() {
-  run<32, false, 1>("A tmem");
-  run<64, false, 1>("A tmem");
-  run<128, false, 1>("A tmem");
-  run<256, false, 1>("A tmem");
-  run<64, false, 2>("A tmem, 2 accum");
-  run<64, false, 4>("A tmem, 4 accum");
-  run<64, true, 1>("A smem");
-  run<128, true, 1>("A smem");
-  run<256, true, 1>("A smem");
+  run<128, 32, false, 1>("A tmem");
+  run<128, 64, false, 1>("A tmem");
+  run<128, 128, false, 1>("A tmem");
+  run<128, 256, false, 1>("A tmem");
+  run<128, 64, false, 2>("A tmem, 2 accum");
+  run<128, 64, false, 4>("A tmem, 4 accum");
+  run<128, 64, true, 1>("A smem");
+  run<128, 128, true, 1>("A smem");
+  run<128, 256, true, 1>("A smem");
+  run<64, 64, true, 1>("A smem");
+  run<64, 128, true, 1>("A smem");
+  run<64, 256, true, 1>("A smem");
   return 0;
 }

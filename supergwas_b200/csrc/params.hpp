@@ -52,6 +52,9 @@ struct DevOut {
   // FP64 refinement list (global k-mer indices), used when EpiParams::refine
   unsigned long long* cand;
   unsigned long long cand_cap;
+  // optional: a tested k-mer counts weight[kmer_offset + local] times in
+  // counters[0] (a row that stands for a run of equal rows)
+  const uint32_t* weight;
 };
 
 enum : unsigned { ERR_TIMEOUT_FULL = 1u, ERR_TIMEOUT_MMA = 2u, ERR_HIT_OVERFLOW = 4u, ERR_CAND_OVERFLOW = 8u };

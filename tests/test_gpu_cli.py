@@ -129,7 +129,7 @@ def test_index_out_matches_build_index(built, mode):
     idx1, idx2 = os.path.join(work, "idx1"), os.path.join(work, "idx2")
     inp = paths["batch"] if mode == "cols" else rows
     r = H.run_cli([paths["samples"], paths["pheno"], inp, paths["ubin"], out, "0", "--log10-thresh-2d", "1",
-                   "--mode", mode, "--index-out", idx1, "--index-2d-out", idx2])
+                   "--mode", mode, "--index-out", idx1, "--index-2d-out", idx2], {"CORR_THRESHOLD": "0"})
     assert r.returncode == 0, r.stderr[-2000:]
     two = O.path_2d(out)
     assert len(H.parse_rows(out)) > 1000 and len(H.parse_rows(two)) > 100
