@@ -236,9 +236,11 @@ const char* kg_last_kernel(const kg_ctx* ctx);
  * adjacent rows (0 when it tested every row).  Batches sorted by bit pattern
  * (src/convert_matrix.cpp:366-368) hold such runs; one row per run is tested,
  * counts once per row of its run in n_tested, and its hit is repeated for
- * every row of the run, so the result is the same as without runs.  Not used
- * when kg_stats outputs are requested; KG_DEDUP=0 in the environment turns
- * it off. */
+ * every row of the run, so the result is the same as without runs.  Used for
+ * pageable host rows (which are staged through the host anyway) when at least
+ * 10% of sampled adjacent rows are equal, never when kg_stats outputs are
+ * requested.  KG_DEDUP=0 in the environment turns it off, KG_DEDUP=1 uses it
+ * for pinned rows too. */
 uint64_t kg_last_unique_rows(const kg_ctx* ctx);
 
 const char* kg_last_error(const kg_ctx* ctx);

@@ -101,6 +101,7 @@ void kg_destroy(kg_ctx* ctx) {
   for (int b = 0; b < NBUF; ++b) {
     dfree(ctx->dChunk[b]);
     if (ctx->hStage[b]) cudaFreeHost(ctx->hStage[b]);
+    if (ctx->hWeight[b]) cudaFreeHost(ctx->hWeight[b]);
     if (ctx->ev_h2d[b]) cudaEventDestroy(ctx->ev_h2d[b]);
     if (ctx->ev_k[b]) cudaEventDestroy(ctx->ev_k[b]);
   }
@@ -215,6 +216,180 @@ int kg_set_structure(kg_ctx* ctx, const double* U, int n, int k, const double* y
 }
 
 }  // extern "C"
+
+namespace kgctx {
+
+// Gathers rows sel[0..cnt) of x into dst (row bytes each), in parallel for
+// large copies.
+void par_gather(void* dst, const uint64_t* x, const uint64_t* sel, uint64_t cnt, size_t row) {
+  auto body = [=](uint64_t a, uint64_t b) {
+    for (uint64_t u = a; u < b; ++u) std::memcpy((char*)dst + u * row, (const char*)x + sel[u] * row, row);
+  };
+  const size_t kMin = (size_t)64 << 20;
+  unsigned nt = std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
+  if (cnt * row < kMin || nt == 1) {
+    body(0, cnt);
+    return;
+  }
+  std::vector<std::thread> th;
+  const uint64_t per = (cnt + nt - 1) / nt;
+  for (unsigned t = 0; t < nt; ++t) {
+    const uint64_t a = t * per, b = std::min<uint64_t>(cnt, a + per);
+    if (a >= b) break;
+    th.emplace_back(body, a, b);
+  }
+  for (auto& t : th) t.join();
+}
+
+bool is_pinned(const void* p) {
+  cudaPointerAttributes attr{};
+  const bool pinned = cudaPointerGetAttributes(&attr, p) == cudaSuccess &&
+                      (attr.type == cudaMemoryTypeHost || attr.type == cudaMemoryTypeManaged);
+  cudaGetLastError();
+  return pinned;
+}
+
+bool use_runs(const uint64_t* x, uint64_t m, uint32_t wpk, bool pageable) {
+  const char* v = std::getenv("KG_DEDUP");
+  if ((v && std::string(v) == "0") || m < 2 || m >= (1ull << 32)) return false;
+  if (v && std::string(v) == "1") return true;
+  if (!pageable || m < 4096) return false;
+  const size_t row = (size_t)wpk * 8;
+  int dups = 0;
+  for (int i = 0; i < 4096; ++i) {
+    const uint64_t j = 1 + (uint64_t)i * (m - 1) / 4096;
+    dups += rows_equal(x + j * wpk, x + (j - 1) * wpk, wpk) ? 1 : 0;
+  }
+  return dups * 10 >= 4096;
+}
+
+uint64_t scan_gather(const uint64_t* x, uint64_t s0, uint64_t cnt, uint32_t wpk, void* dst,
+                     const std::vector<unsigned long long>& bounds, std::vector<uint64_t>& first,
+                     std::vector<uint32_t>& len, std::vector<StageSeg>& segs) {
+  const size_t row = (size_t)wpk * 8;
+  unsigned nt = std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency()));
+  if (cnt < (1u << 16)) nt = 1;
+  std::vector<std::vector<uint64_t>> st(nt);
+  // one pass: thread t scans rows [a, b) and copies each run's first row to
+  // its own slice of dst (rows a - s0 onwards)
+  auto scan = [&](unsigned t) {
+    const uint64_t a = s0 + cnt * t / nt, b = s0 + cnt * (t + 1) / nt;
+    auto bd = std::lower_bound(bounds.begin(), bounds.end(), (unsigned long long)a);
+    char* out = (char*)dst + (a - s0) * row;
+    std::vector<uint64_t>& v = st[t];
+    v.reserve((b - a) / 2 + 16);
+    for (uint64_t i = a; i < b; ++i) {
+      bool start = i == s0 || !rows_equal(x + i * wpk, x + (i - 1) * wpk, wpk);
+      while (bd != bounds.end() && *bd < i) ++bd;
+      if (bd != bounds.end() && *bd == i) start = true;
+      if (start) {
+        std::memcpy(out, x + i * wpk, row);
+        out += row;
+        v.push_back(i);
+      }
+    }
+  };
+  if (nt == 1) {
+    scan(0);
+  } else {
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t) th.emplace_back(scan, t);
+    for (auto& t : th) t.join();
+  }
+  const size_t base = first.size();
+  segs.clear();
+  for (unsigned t = 0; t < nt; ++t) {
+    if (!st[t].empty()) segs.push_back({cnt * t / nt, (uint64_t)st[t].size()});
+    first.insert(first.end(), st[t].begin(), st[t].end());
+  }
+  const uint64_t nu = first.size() - base;
+  len.resize(base + nu);
+  for (uint64_t u = 0; u < nu; ++u)
+    len[base + u] = (uint32_t)((u + 1 < nu ? first[base + u + 1] : s0 + cnt) - first[base + u]);
+  return nu;
+}
+
+bool find_runs(kg_ctx* ctx, const uint64_t* x, uint64_t m, uint32_t wpk, const std::vector<unsigned long long>& bounds,
+               bool pageable) {
+  if (!use_runs(x, m, wpk, pageable)) return false;
+  const char* v = std::getenv("KG_DEDUP");
+  const bool force = v && std::string(v) == "1";
+  const size_t row = (size_t)wpk * 8;
+  (void)row;
+  auto same = [&](uint64_t i) { return rows_equal(x + i * wpk, x + (i - 1) * wpk, wpk); };
+  unsigned nt = std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency()));
+  if (m < (1u << 16)) nt = 1;
+  std::vector<std::vector<uint64_t>> starts(nt);
+  auto scan = [&](unsigned t) {
+    const uint64_t a = m * t / nt, b = m * (t + 1) / nt;
+    // the bounds (shard starts) also start runs
+    auto bd = std::lower_bound(bounds.begin(), bounds.end(), (unsigned long long)a);
+    for (uint64_t i = a; i < b; ++i) {
+      bool start = i == 0 || !same(i);
+      while (bd != bounds.end() && *bd < i) ++bd;
+      if (bd != bounds.end() && *bd == i) start = true;
+      if (start) starts[t].push_back(i);
+    }
+  };
+  if (nt == 1) {
+    scan(0);
+  } else {
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t) th.emplace_back(scan, t);
+    for (auto& t : th) t.join();
+  }
+  size_t nu = 0;
+  for (auto& s : starts) nu += s.size();
+  if (force ? nu == m : nu * 10 > m * 9) return false;
+  ctx->run_first.clear();
+  ctx->run_first.reserve(nu);
+  for (auto& s : starts) ctx->run_first.insert(ctx->run_first.end(), s.begin(), s.end());
+  ctx->run_len.resize(nu);
+  for (size_t u = 0; u < nu; ++u)
+    ctx->run_len[u] = (uint32_t)((u + 1 < nu ? ctx->run_first[u + 1] : m) - ctx->run_first[u]);
+  return true;
+}
+
+int upload_run_lengths(kg_ctx* ctx, cudaStream_t st) {
+  const size_t nu = ctx->run_len.size();
+  if (ctx->weight_cap < nu) {
+    dfree(ctx->dWeight);
+    ctx->weight_cap = 0;
+    KG_CUDA(cudaMalloc((void**)&ctx->dWeight, nu * sizeof(uint32_t)), "cudaMalloc(run lengths)");
+    ctx->weight_cap = nu;
+  }
+  KG_CUDA(cudaMemcpyAsync(ctx->dWeight, ctx->run_len.data(), nu * sizeof(uint32_t), cudaMemcpyHostToDevice, st),
+          "copy run lengths");
+  ctx->cur_weight = ctx->dWeight;
+  ctx->unique_rows = nu;
+  return KG_OK;
+}
+
+void expand_runs(const kg_ctx* ctx, std::vector<kg_hit>& hits) {
+  std::vector<kg_hit> all;
+  for (const kg_hit& h : hits) {
+    const uint64_t f = ctx->run_first[h.kmer], e = f + ctx->run_len[h.kmer];
+    for (uint64_t i = f; i < e; ++i) {
+      all.push_back(h);
+      all.back().kmer = i;
+    }
+  }
+  hits.swap(all);
+}
+
+void expand_runs(const kg_ctx* ctx, std::vector<kg_phit>& hits) {
+  std::vector<kg_phit> all;
+  for (const kg_phit& h : hits) {
+    const uint64_t f = ctx->run_first[h.kmer], e = f + ctx->run_len[h.kmer];
+    for (uint64_t i = f; i < e; ++i) {
+      all.push_back(h);
+      all.back().kmer = i;
+    }
+  }
+  hits.swap(all);
+}
+
+}  // namespace kgctx
 
 namespace {
 
@@ -363,87 +538,18 @@ void par_memcpy(void* dst, const void* src, size_t bytes) {
   for (auto& t : th) t.join();
 }
 
-// Gathers rows sel[0..cnt) of x into dst (row bytes each), in parallel for
-// large copies.
-void par_gather(void* dst, const uint64_t* x, const uint64_t* sel, uint64_t cnt, size_t row) {
-  auto body = [=](uint64_t a, uint64_t b) {
-    for (uint64_t u = a; u < b; ++u) std::memcpy((char*)dst + u * row, (const char*)x + sel[u] * row, row);
-  };
-  const size_t kMin = (size_t)64 << 20;
-  unsigned nt = std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
-  if (cnt * row < kMin || nt == 1) {
-    body(0, cnt);
-    return;
-  }
-  std::vector<std::thread> th;
-  const uint64_t per = (cnt + nt - 1) / nt;
-  for (unsigned t = 0; t < nt; ++t) {
-    const uint64_t a = t * per, b = std::min<uint64_t>(cnt, a + per);
-    if (a >= b) break;
-    th.emplace_back(body, a, b);
-  }
-  for (auto& t : th) t.join();
-}
-
-// Runs of equal adjacent rows.  Real batches are sorted by bit pattern
-// (src/convert_matrix.cpp:366-368), so equal rows sit next to each other; an
-// equal row has equal statistics, so one row per run is tested and counts as
-// many tested k-mers as the run has rows.  4096 sampled adjacent pairs decide
-// whether the full scan can pay (at least 10 % repeats); the runs are used
-// when they save at least 10 % of the rows.  KG_DEDUP=0 switches this off,
-// KG_DEDUP=1 uses the runs whenever any row repeats.
-bool find_runs(kg_ctx* ctx, const uint64_t* x, uint64_t m, uint32_t wpk) {
-  const char* v = std::getenv("KG_DEDUP");
-  const bool off = v && std::string(v) == "0", force = v && std::string(v) == "1";
-  if (off || m < 2 || m >= (1ull << 32)) return false;
-  const size_t row = (size_t)wpk * 8;
-  auto same = [&](uint64_t i) { return std::memcmp(x + i * wpk, x + (i - 1) * wpk, row) == 0; };
-  if (!force) {
-    if (m < 4096) return false;
-    int dups = 0;
-    for (int i = 0; i < 4096; ++i) dups += same(1 + (uint64_t)i * (m - 1) / 4096) ? 1 : 0;
-    if (dups * 10 < 4096) return false;
-  }
-  unsigned nt = std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency()));
-  if (m < (1u << 16)) nt = 1;
-  std::vector<std::vector<uint64_t>> starts(nt);
-  auto scan = [&](unsigned t) {
-    const uint64_t a = m * t / nt, b = m * (t + 1) / nt;
-    for (uint64_t i = a; i < b; ++i)
-      if (i == 0 || !same(i)) starts[t].push_back(i);
-  };
-  if (nt == 1) {
-    scan(0);
-  } else {
-    std::vector<std::thread> th;
-    for (unsigned t = 0; t < nt; ++t) th.emplace_back(scan, t);
-    for (auto& t : th) t.join();
-  }
-  size_t nu = 0;
-  for (auto& s : starts) nu += s.size();
-  if (force ? nu == m : nu * 10 > m * 9) return false;
-  ctx->run_first.clear();
-  ctx->run_first.reserve(nu);
-  for (auto& s : starts) ctx->run_first.insert(ctx->run_first.end(), s.begin(), s.end());
-  ctx->run_len.resize(nu);
-  for (size_t u = 0; u < nu; ++u)
-    ctx->run_len[u] = (uint32_t)((u + 1 < nu ? ctx->run_first[u + 1] : m) - ctx->run_first[u]);
-  return true;
-}
-
-// sel (optional): test rows sel[0..m) of xbits, gathered on the host.
-int run_host_once(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t wpk, bool stats,
-                  const uint64_t* sel = nullptr) {
+// One pass of the rows through the chunked host-to-device pipeline.  With
+// `runs`, each chunk is scanned for runs of equal rows while it is staged and
+// only the first row of each run is copied and tested, weighted by its run's
+// length (ctx->run_first / run_len / unique_rows describe the runs).
+int run_host_once(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t wpk, bool stats, bool runs) {
   const size_t row = (size_t)wpk * 8;
   size_t want = (size_t)512 << 20;
   if (const char* v = std::getenv("KG_CHUNK_MB")) want = (size_t)std::max(1, std::atoi(v)) << 20;
   uint64_t per = std::max<uint64_t>(1, want / row);
   if (per > m) per = m;
   const size_t bytes = (size_t)per * row;
-  cudaPointerAttributes attr{};
-  bool pinned = !sel && cudaPointerGetAttributes(&attr, xbits) == cudaSuccess &&
-                (attr.type == cudaMemoryTypeHost || attr.type == cudaMemoryTypeManaged);
-  cudaGetLastError();
+  const bool pinned = !runs && is_pinned(xbits);
   if (ctx->chunk_bytes < bytes) {
     for (int b = 0; b < NBUF; ++b) {
       dfree(ctx->dChunk[b]);
@@ -457,32 +563,72 @@ int run_host_once(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t wpk, 
   if (!pinned)
     for (int b = 0; b < NBUF; ++b)
       if (!ctx->hStage[b]) KG_CUDA(cudaHostAlloc(&ctx->hStage[b], ctx->chunk_bytes, cudaHostAllocDefault), "cudaHostAlloc");
+  if (runs) {
+    ctx->run_first.clear();
+    ctx->run_len.clear();
+    if (ctx->weight_cap < m) {
+      dfree(ctx->dWeight);
+      ctx->weight_cap = 0;
+      KG_CUDA(cudaMalloc((void**)&ctx->dWeight, m * sizeof(uint32_t)), "cudaMalloc(run lengths)");
+      ctx->weight_cap = m;
+    }
+    if (ctx->hweight_cap < per) {
+      for (int b = 0; b < NBUF; ++b) {
+        if (ctx->hWeight[b]) cudaFreeHost(ctx->hWeight[b]);
+        ctx->hWeight[b] = nullptr;
+      }
+      ctx->hweight_cap = 0;
+      for (int b = 0; b < NBUF; ++b)
+        KG_CUDA(cudaHostAlloc((void**)&ctx->hWeight[b], per * sizeof(uint32_t), cudaHostAllocDefault), "cudaHostAlloc");
+      ctx->hweight_cap = per;
+    }
+    ctx->cur_weight = ctx->dWeight;
+  }
   KG_CUDA(cudaMemsetAsync(ctx->dCounters, 0, 4 * sizeof(unsigned long long), ctx->stream), "memset");
   const uint64_t nch = (m + per - 1) / per;
+  uint64_t u0 = 0;  // runs before this chunk
+  std::vector<StageSeg> segs;
   for (uint64_t i = 0; i < nch; ++i) {
     const int b = (int)(i % NBUF);
     const uint64_t s = i * per, cnt = std::min<uint64_t>(per, m - s);
     const size_t nb = (size_t)cnt * row;
+    uint64_t rows = cnt, offset = s;
     const char* src = (const char*)xbits + (size_t)s * row;
     if (i >= (uint64_t)NBUF) {
       // buffer b was last read by chunk i-NBUF's copy and kernel
       KG_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_k[b], 0), "wait");
       if (!pinned) KG_CUDA(cudaEventSynchronize(ctx->ev_h2d[b]), "sync");
     }
-    if (sel) {
-      par_gather(ctx->hStage[b], xbits, sel + s, cnt, row);
-      src = (const char*)ctx->hStage[b];
-    } else if (!pinned) {
-      par_memcpy(ctx->hStage[b], src, nb);
-      src = (const char*)ctx->hStage[b];
+    if (runs) {
+      rows = scan_gather(xbits, s, cnt, wpk, ctx->hStage[b], {}, ctx->run_first, ctx->run_len, segs);
+      std::memcpy(ctx->hWeight[b], ctx->run_len.data() + u0, rows * sizeof(uint32_t));
+      KG_CUDA(cudaMemcpyAsync(ctx->dWeight + u0, ctx->hWeight[b], rows * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                              ctx->copy_stream),
+              "H2D");
+      // the threads' slices of the staging buffer, back to back on the device
+      uint64_t d = 0;
+      for (const StageSeg& g : segs) {
+        KG_CUDA(cudaMemcpyAsync((char*)ctx->dChunk[b] + d * row, (const char*)ctx->hStage[b] + g.stage_row * row,
+                                g.rows * row, cudaMemcpyHostToDevice, ctx->copy_stream),
+                "H2D");
+        d += g.rows;
+      }
+      offset = u0;
+      u0 += rows;
+    } else {
+      if (!pinned) {
+        par_memcpy(ctx->hStage[b], src, nb);
+        src = (const char*)ctx->hStage[b];
+      }
+      KG_CUDA(cudaMemcpyAsync(ctx->dChunk[b], src, nb, cudaMemcpyHostToDevice, ctx->copy_stream), "H2D");
     }
-    KG_CUDA(cudaMemcpyAsync(ctx->dChunk[b], src, nb, cudaMemcpyHostToDevice, ctx->copy_stream), "H2D");
     KG_CUDA(cudaEventRecord(ctx->ev_h2d[b], ctx->copy_stream), "record");
     KG_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_h2d[b], 0), "wait");
-    int rc = launch_one(ctx, ctx->dChunk[b], cnt, wpk, s, stats, ctx->stream);
+    int rc = launch_one(ctx, ctx->dChunk[b], rows, wpk, offset, stats, ctx->stream);
     if (rc) return rc;
     KG_CUDA(cudaEventRecord(ctx->ev_k[b], ctx->stream), "record");
   }
+  if (runs) ctx->unique_rows = u0;
   KG_CUDA(cudaMemcpyAsync(ctx->counters, ctx->dCounters, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                           ctx->stream),
           "copy counters");
@@ -508,48 +654,24 @@ int kg_run_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t wpk, kg
   if ((rc = ensure_cand(ctx, std::max<unsigned long long>(ctx->cand_cap, 1ull << 20)))) return rc;
   std::memset(ctx->counters, 0, sizeof(ctx->counters));
   // per-k-mer outputs are kept for every row, so runs are only used without them
-  const bool dedup = !stats && find_runs(ctx, xbits, m, wpk);
-  const uint64_t* sel = nullptr;
-  uint64_t mt = m;  // rows tested on the device
-  if (dedup) {
-    mt = ctx->run_first.size();
-    sel = ctx->run_first.data();
-    if (ctx->weight_cap < mt) {
-      dfree(ctx->dWeight);
-      ctx->weight_cap = 0;
-      KG_CUDA(cudaMalloc((void**)&ctx->dWeight, mt * sizeof(uint32_t)), "cudaMalloc(run lengths)");
-      ctx->weight_cap = mt;
-    }
-    KG_CUDA(cudaMemcpyAsync(ctx->dWeight, ctx->run_len.data(), mt * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                            ctx->stream),
-            "copy run lengths");
-    ctx->cur_weight = ctx->dWeight;
-    ctx->unique_rows = mt;
-  }
+  const bool runs = !stats && use_runs(xbits, m, wpk, !is_pinned(xbits));
   struct Reset {
     kg_ctx* c;
     ~Reset() { c->cur_weight = nullptr; }
   } reset{ctx};
-  if (mt) {
-    if ((rc = run_host_once(ctx, xbits, mt, wpk, stats, sel))) return rc;
+  if (m) {
+    if ((rc = run_host_once(ctx, xbits, m, wpk, stats, runs))) return rc;
     for (int retry = 0; retry < 8 && (ctx->counters[2] & (kg::ERR_HIT_OVERFLOW | kg::ERR_CAND_OVERFLOW)); ++retry) {
       if ((ctx->counters[2] & kg::ERR_HIT_OVERFLOW) && (rc = ensure_hits(ctx, ctx->counters[1]))) return rc;
       if ((ctx->counters[2] & kg::ERR_CAND_OVERFLOW) && (rc = ensure_cand(ctx, 4 * ctx->cand_cap))) return rc;
-      if ((rc = run_host_once(ctx, xbits, mt, wpk, stats, sel))) return rc;
+      if ((rc = run_host_once(ctx, xbits, m, wpk, stats, runs))) return rc;
     }
   }
+  const uint64_t mt = runs ? ctx->unique_rows : m;  // rows tested on the device
   if ((rc = collect(ctx, mt, res, st, stats))) return rc;
-  if (dedup) {
+  if (runs) {
     // every row of a run gets its run's row, in row order
-    std::vector<kg_hit> all;
-    for (const kg_hit& h : ctx->hits) {
-      const uint64_t f = ctx->run_first[h.kmer], e = f + ctx->run_len[h.kmer];
-      for (uint64_t i = f; i < e; ++i) {
-        all.push_back(h);
-        all.back().kmer = i;
-      }
-    }
-    ctx->hits.swap(all);
+    expand_runs(ctx, ctx->hits);
     if (res) {
       res->n_kmers = m;
       res->n_hits = ctx->hits.size();

@@ -113,6 +113,7 @@ kg::DevOutMP dev_out(kg_ctx* ctx, unsigned long long offset) {
   O.n_shards = M.n_shards;
   O.n_pheno = M.np;
   O.kmer_offset = offset;
+  O.weight = ctx->cur_weight;
   return O;
 }
 
@@ -464,13 +465,33 @@ int kg_run_multi_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t w
   int rc = check_multi(ctx, xbits, m, wpk);
   if (rc) return rc;
   if ((rc = set_shards(ctx, shard_start, n_shards, m))) return rc;
+  cudaStream_t st = ctx->stream;
+  // runs of equal rows (as in kg_run_host); a shard start also starts a run,
+  // so each tested row belongs to one shard
+  ctx->unique_rows = 0;
+  const bool dedup = find_runs(ctx, xbits, m, wpk, M.shard_host, !is_pinned(xbits));
+  const uint64_t* sel = nullptr;
+  const uint64_t m_all = m;
+  if (dedup) {
+    std::vector<uint64_t> us(M.shard_host.size());
+    for (size_t i = 0; i < us.size(); ++i)
+      us[i] = (uint64_t)(std::lower_bound(ctx->run_first.begin(), ctx->run_first.end(), M.shard_host[i]) -
+                         ctx->run_first.begin());
+    m = ctx->run_first.size();
+    sel = ctx->run_first.data();
+    if ((rc = set_shards(ctx, us.data(), (int)us.size(), m))) return rc;
+    if ((rc = upload_run_lengths(ctx, st))) return rc;
+  }
+  struct Reset {
+    kg_ctx* c;
+    ~Reset() { c->cur_weight = nullptr; }
+  } reset{ctx};
   if ((rc = ensure_multi_out(ctx, M.n_shards, std::max<unsigned long long>(M.hit_cap, 1ull << 16)))) return rc;
   if (!ctx->dCand || ctx->cand_cap < (1ull << 20)) {
     dfree(ctx->dCand);
     KG_CUDA(cudaMalloc((void**)&ctx->dCand, (1ull << 20) * sizeof(unsigned long long)), "cudaMalloc(candidates)");
     ctx->cand_cap = 1ull << 20;
   }
-  cudaStream_t st = ctx->stream;
   KG_CUDA(cudaMemcpyAsync(M.dShard, M.shard_host.data(), M.shard_host.size() * sizeof(unsigned long long),
                           cudaMemcpyHostToDevice, st),
           "copy shards");
@@ -486,8 +507,8 @@ int kg_run_multi_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t w
     if (per > m) per = m;
     const size_t bytes = (size_t)per * row;
     cudaPointerAttributes attr{};
-    const bool pinned = m == 0 || (cudaPointerGetAttributes(&attr, xbits) == cudaSuccess &&
-                                   (attr.type == cudaMemoryTypeHost || attr.type == cudaMemoryTypeManaged));
+    const bool pinned = !sel && (m == 0 || (cudaPointerGetAttributes(&attr, xbits) == cudaSuccess &&
+                                            (attr.type == cudaMemoryTypeHost || attr.type == cudaMemoryTypeManaged)));
     cudaGetLastError();
     if (ctx->chunk_bytes < bytes) {
       for (int b = 0; b < NBUF; ++b) {
@@ -513,7 +534,10 @@ int kg_run_multi_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t w
         KG_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_k[b], 0), "wait");
         if (!pinned) KG_CUDA(cudaEventSynchronize(ctx->ev_h2d[b]), "sync");
       }
-      if (!pinned) {
+      if (sel) {
+        par_gather(ctx->hStage[b], xbits, sel + s0, cnt, row);
+        src = (const char*)ctx->hStage[b];
+      } else if (!pinned) {
         std::memcpy(ctx->hStage[b], src, nb);
         src = (const char*)ctx->hStage[b];
       }
@@ -541,7 +565,16 @@ int kg_run_multi_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t w
   }
   drop_graph(M);
   M.g_x = nullptr;
-  return collect_multi(ctx, m, res);
+  if ((rc = collect_multi(ctx, m, res))) return rc;
+  if (dedup) {
+    expand_runs(ctx, M.hits);
+    if (res) {
+      res->n_kmers = m_all;
+      res->n_hits = M.hits.size();
+      res->hits = M.hits.data();
+    }
+  }
+  return KG_OK;
 }
 
 }  // extern "C"

@@ -153,6 +153,8 @@ struct kg_ctx {
   std::vector<uint32_t> run_len;
   uint32_t* dWeight = nullptr;
   size_t weight_cap = 0;
+  uint32_t* hWeight[kgctx::NBUF] = {};  // pinned staging of one chunk's run lengths
+  size_t hweight_cap = 0;
   const uint32_t* cur_weight = nullptr;  // set while a deduplicated run is in flight
   uint64_t unique_rows = 0;              // rows the last kg_run_host tested (0: no deduplication)
   // many phenotypes
@@ -185,3 +187,50 @@ struct kg_ctx {
 namespace kgctx {
 void free_multi(kg_ctx* ctx);  // capi_multi.cpp
 }  // namespace kgctx
+
+namespace kgctx {
+
+// Runs of equal adjacent host rows.  Real batches are sorted by bit pattern
+// (src/convert_matrix.cpp:366-368), so equal rows sit next to each other; an
+// equal row has equal statistics, so one row per run is tested and counts as
+// many tested k-mers as the run has rows.
+//
+// use_runs: whether to test one row per run.  Finding the runs reads every
+// row on the host, which pays only where the rows are copied through the host
+// anyway (pageable memory): there, at least 10 % of 4096 sampled adjacent
+// pairs must be equal.  KG_DEDUP=0 never, KG_DEDUP=1 always (pinned too).
+bool use_runs(const uint64_t* x, uint64_t m, uint32_t wpk, bool pageable);
+inline bool rows_equal(const uint64_t* a, const uint64_t* b, uint32_t wpk) {
+  uint64_t d = 0;
+  for (uint32_t w = 0; w < wpk; ++w) d |= a[w] ^ b[w];
+  return d == 0;
+}
+// A slice of a staging buffer: `rows` rows from row `stage_row` on.
+struct StageSeg {
+  uint64_t stage_row, rows;
+};
+// Rows [s0, s0 + cnt) of x in one pass: a row starts a run when it is the
+// first of the range, differs from its predecessor or is in `bounds`
+// (ascending row indices).  Host threads copy the first row of each run into
+// their own slices of dst (listed in segs, in row order), the runs' first rows
+// and lengths are appended to first / len; returns the number of runs.
+uint64_t scan_gather(const uint64_t* x, uint64_t s0, uint64_t cnt, uint32_t wpk, void* dst,
+                     const std::vector<unsigned long long>& bounds, std::vector<uint64_t>& first,
+                     std::vector<uint32_t>& len, std::vector<StageSeg>& segs);
+// All runs of x at once (kg_run_multi_host): fills ctx->run_first / run_len
+// and returns true when use_runs holds and the runs save at least 10 % of the
+// rows; `bounds` (shard starts) also start runs.
+bool find_runs(kg_ctx* ctx, const uint64_t* x, uint64_t m, uint32_t wpk, const std::vector<unsigned long long>& bounds,
+               bool pageable);
+bool is_pinned(const void* p);
+// Copies the run lengths to the device and makes them the tested-count
+// weights of the following launches (ctx->cur_weight).
+int upload_run_lengths(kg_ctx* ctx, cudaStream_t st);
+// Gathers rows sel[0..cnt) of x into dst (row bytes each).
+void par_gather(void* dst, const uint64_t* x, const uint64_t* sel, uint64_t cnt, size_t row);
+// Repeats each hit of a distinct row for every row of its run, in row order.
+void expand_runs(const kg_ctx* ctx, std::vector<kg_hit>& hits);
+void expand_runs(const kg_ctx* ctx, std::vector<kg_phit>& hits);
+
+}  // namespace kgctx
+

@@ -627,9 +627,15 @@ __device__ __forceinline__ void mp_emit_rare(const DevOutMP& O, int p, unsigned 
 __device__ __forceinline__ void mp_emit(const DevOutMP& O, int p, unsigned long long gk, int shard, unsigned match,
                                         bool leader, bool tested, bool hit, bool cand, double T, double pv,
                                         double effect) {
-  const unsigned tm = __ballot_sync(0xffffffffu, tested);
-  if (leader && (tm & match))
-    atomicAdd(O.tested + (size_t)shard * O.n_pheno + p, (unsigned long long)__popc(tm & match));
+  if (O.weight) {
+    // the lanes of one shard (match) add their rows' weights
+    const unsigned tot = __reduce_add_sync(match, tested ? O.weight[gk] : 0u);
+    if (leader && tot) atomicAdd(O.tested + (size_t)shard * O.n_pheno + p, (unsigned long long)tot);
+  } else {
+    const unsigned tm = __ballot_sync(0xffffffffu, tested);
+    if (leader && (tm & match))
+      atomicAdd(O.tested + (size_t)shard * O.n_pheno + p, (unsigned long long)__popc(tm & match));
+  }
   mp_emit_rare(O, p, gk, shard, hit, cand, T, pv, effect);
 }
 

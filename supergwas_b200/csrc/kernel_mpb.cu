@@ -363,6 +363,7 @@ __global__ void __launch_bounds__(mb_threads(NP * PPG), 1)
           const bool valid = local < m;
           const unsigned long long gk = O.kmer_offset + local;
           const int shard = mp_shard(O, gk);
+          const uint32_t wt = O.weight && valid ? O.weight[gk] : 1u;  // rows this row stands for
           if (__any_sync(0xffffffffu, shard != cur)) {
             mb_flush<PPG>(O, g, cur, cnt);
             cur = shard;
@@ -439,7 +440,7 @@ __global__ void __launch_bounds__(mb_threads(NP * PPG), 1)
             bool tested, hit, cand;
             double T, pv, effect;
             mp_eval(P, valid, c, ss, gs, ey, tested, hit, cand, T, pv, effect);
-            cnt[pp] += tested ? 1u : 0u;
+            cnt[pp] += tested ? wt : 0u;
             if (__any_sync(0xffffffffu, hit || cand)) mp_emit_rare(O, p, gk, shard, hit, cand, T, pv, effect);
           }
         }

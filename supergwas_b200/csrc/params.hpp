@@ -84,6 +84,9 @@ struct DevOutMP {
   int n_shards;
   int n_pheno;
   unsigned long long kmer_offset;
+  // optional: a tested (k-mer, phenotype) counts weight[global k-mer] times
+  // (a row that stands for a run of equal rows)
+  const uint32_t* weight;
 };
 
 // Outputs of the 2-D pair test (kernel_pairs.cu).

@@ -82,3 +82,31 @@ def test_no_runs_no_scan(built):
         g.set_structure(ds.U, ds.y)
         g.run_host(ds.packed_overlap())
         assert g.last_unique_rows() == 0
+
+
+@pytest.mark.parametrize("kernel", ["stationary", "streamed"])
+def test_multi_runs_match_every_row(built, monkeypatch, kernel):
+    """kg_run_multi_host with runs: per-(shard, phenotype) counts and rows as
+    for every row; a shard start also starts a run, so a run of equal rows
+    that crosses a shard boundary is counted in both shards."""
+    from test_gpu_multi import make_batch
+    if kernel == "streamed":
+        monkeypatch.setenv("KG_MP_STREAMED", "1")
+    n_all, m = 1000, 6000
+    packed, phenos = make_batch(n_all, m, 5, (16, 4), seed=91, wpk=16)
+    packed = _distinct(packed)
+    X2, reps = _runs(packed, 13, 17, 5000)
+    m2 = X2.shape[0]
+    # shard starts in the middle of runs, at a run start, and an empty shard
+    first = np.concatenate([[0], np.cumsum(reps)[:-1]])
+    shards = np.array([0, first[17] + 100, first[40], first[40], m2 - 3], dtype=np.uint64)
+    with api.Kgwas(corr_threshold=0.2, log10_thresh=1.0) as g:
+        g.set_phenotypes(phenos, n_all)
+        t_runs, h_runs = g.run_multi_host(X2, shards)
+        assert 0 < g.last_unique_rows() < m2
+        monkeypatch.setenv("KG_DEDUP", "0")
+        t_all, h_all = g.run_multi_host(X2, shards)
+        assert g.last_unique_rows() == 0
+    assert np.array_equal(t_runs, t_all)
+    assert np.array_equal(h_runs, h_all)
+    assert h_runs.shape[0] > 0

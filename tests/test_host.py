@@ -267,3 +267,50 @@ def test_index_out_option_errors(built, tmp_path):
         r = H.run_cli([*base, *extra])
         assert r.returncode == 1 and msg in r.stderr, (extra, r.stderr)
 
+
+def _runs_lib():
+    out = os.path.join(HERE, "native", "_build", "libruns_check.so")
+    src = os.path.join(HERE, "native", "runs_check.cpp")
+    deps = [src, build.LIB, os.path.join(build.CSRC, "ctx.hpp")]
+    if not os.path.exists(out) or any(os.path.getmtime(d) > os.path.getmtime(out) for d in deps):
+        os.makedirs(os.path.dirname(out), exist_ok=True)
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-o", out, src, "-I/usr/local/cuda/include",
+                        "-L" + build.LIB_DIR, "-lkgwas_cuda", "-Wl,-rpath," + build.LIB_DIR], check=True)
+    L = ctypes.CDLL(out)
+    vp = ctypes.c_void_p
+    L.runs_check.argtypes = [vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, vp, ctypes.c_int, vp, vp, vp]
+    L.runs_check.restype = ctypes.c_uint64
+    return L
+
+
+@pytest.mark.parametrize("m,wpk,s0,cnt", [(300_000, 16, 0, 300_000), (300_000, 2, 1234, 200_001),
+                                          (5_000, 4, 10, 4000)])
+def test_run_finder(built, m, wpk, s0, cnt):
+    """The host scan behind runs of equal rows (kgctx::scan_gather): a row
+    starts a run at the range start, where it differs from its predecessor,
+    and at every bound; each run's first row reaches the device in row order."""
+    rng = np.random.default_rng(m + wpk)
+    base = rng.integers(0, 2**63, size=(m // 2, wpk), dtype=np.uint64)
+    k = base[1::7].shape[0]
+    base[0:7 * k:7] = base[1::7]                       # neighbouring runs of the same row merge
+    reps = rng.integers(1, 6, size=base.shape[0])
+    X = np.ascontiguousarray(np.repeat(base, reps, axis=0)[:m])
+    assert X.shape[0] == m >= s0 + cnt
+    bounds = np.unique(np.r_[rng.integers(s0, s0 + cnt, size=9), s0 + 5, s0 + cnt + 3]).astype(np.uint64)
+    rows = np.arange(s0, s0 + cnt)
+    diff = np.r_[True, np.any(X[rows[1:]] != X[rows[1:] - 1], axis=1)]
+    start = diff | np.isin(rows, bounds)
+    exp_first = rows[start]
+    exp_len = np.diff(np.r_[exp_first, s0 + cnt])
+    L = _runs_lib()
+    first = np.zeros(cnt, np.uint64)
+    lens = np.zeros(cnt, np.uint32)
+    out = np.zeros((cnt, wpk), np.uint64)
+    nu = L.runs_check(X.ctypes.data, ctypes.c_uint64(s0), ctypes.c_uint64(cnt), ctypes.c_uint32(wpk),
+                      bounds.ctypes.data, ctypes.c_int(bounds.size), first.ctypes.data, lens.ctypes.data,
+                      out.ctypes.data)
+    assert nu == exp_first.size
+    assert np.array_equal(first[:nu], exp_first)
+    assert np.array_equal(lens[:nu], exp_len)
+    assert np.array_equal(out[:nu], X[exp_first])
+
