@@ -219,6 +219,24 @@ int kg_set_structure(kg_ctx* ctx, const double* U, int n, int k, const double* y
 
 namespace kgctx {
 
+// Copy in up to 8 host threads (copies of 64 MB or more).
+void par_memcpy(void* dst, const void* src, size_t bytes) {
+  const size_t kMin = (size_t)64 << 20;
+  unsigned nt = std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
+  if (bytes < kMin || nt == 1) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t per = (bytes + nt - 1) / nt;
+  for (unsigned t = 0; t < nt; ++t) {
+    const size_t a = t * per, b = std::min(bytes, a + per);
+    if (a >= b) break;
+    th.emplace_back([=] { std::memcpy((char*)dst + a, (const char*)src + a, b - a); });
+  }
+  for (auto& t : th) t.join();
+}
+
 // Gathers rows sel[0..cnt) of x into dst (row bytes each), in parallel for
 // large copies.
 void par_gather(void* dst, const uint64_t* x, const uint64_t* sel, uint64_t cnt, size_t row) {
@@ -521,22 +539,6 @@ bool want_stats(const kg_stats* st) {
   return st && (st->tested || st->chisq || st->pval || st->effect || st->mlog10p || st->xxM || st->xyM || st->cor);
 }
 
-void par_memcpy(void* dst, const void* src, size_t bytes) {
-  const size_t kMin = (size_t)64 << 20;
-  unsigned nt = std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
-  if (bytes < kMin || nt == 1) {
-    std::memcpy(dst, src, bytes);
-    return;
-  }
-  std::vector<std::thread> th;
-  const size_t per = (bytes + nt - 1) / nt;
-  for (unsigned t = 0; t < nt; ++t) {
-    const size_t a = t * per, b = std::min(bytes, a + per);
-    if (a >= b) break;
-    th.emplace_back([=] { std::memcpy((char*)dst + a, (const char*)src + a, b - a); });
-  }
-  for (auto& t : th) t.join();
-}
 
 // One pass of the rows through the chunked host-to-device pipeline.  With
 // `runs`, each chunk is scanned for runs of equal rows while it is staged and

@@ -538,7 +538,7 @@ int kg_run_multi_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t w
         par_gather(ctx->hStage[b], xbits, sel + s0, cnt, row);
         src = (const char*)ctx->hStage[b];
       } else if (!pinned) {
-        std::memcpy(ctx->hStage[b], src, nb);
+        par_memcpy(ctx->hStage[b], src, nb);
         src = (const char*)ctx->hStage[b];
       }
       KG_CUDA(cudaMemcpyAsync(ctx->dChunk[b], src, nb, cudaMemcpyHostToDevice, ctx->copy_stream), "H2D");

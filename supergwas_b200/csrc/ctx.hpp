@@ -226,6 +226,8 @@ bool is_pinned(const void* p);
 // Copies the run lengths to the device and makes them the tested-count
 // weights of the following launches (ctx->cur_weight).
 int upload_run_lengths(kg_ctx* ctx, cudaStream_t st);
+// Host copies in up to 8 threads (for 64 MB or more).
+void par_memcpy(void* dst, const void* src, size_t bytes);
 // Gathers rows sel[0..cnt) of x into dst (row bytes each).
 void par_gather(void* dst, const uint64_t* x, const uint64_t* sel, uint64_t cnt, size_t row);
 // Repeats each hit of a distinct row for every row of its run, in row order.
