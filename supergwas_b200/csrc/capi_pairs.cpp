@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -39,6 +40,64 @@ int ensure_pair_cand(kg_ctx* ctx, unsigned long long cap) {
   KG_CUDA(cudaMalloc((void**)&ctx->dCand, cap * sizeof(unsigned long long)), "cudaMalloc(candidates)");
   ctx->cand_cap = cap;
   return KG_OK;
+}
+
+// Sorts the emitted pairs by (a, b).  a lies in the task's row range
+// [row_start, row_end): a counting sort on a, then each row's few pairs
+// sorted by b.  The scatter is bound by cache misses, so host threads each
+// take a block of rows with about the same number of pairs, scatter the pairs
+// of their rows and sort those rows.  A range much wider than the number of
+// pairs falls back to a comparison sort.
+void sort_pairs(std::vector<kg_pair>& v, uint64_t row_start, uint64_t row_end) {
+  auto less = [](const kg_pair& x, const kg_pair& y) { return x.a != y.a ? x.a < y.a : x.b < y.b; };
+  const size_t n = v.size();
+  if (n < 2) return;
+  const uint64_t R = row_end > row_start ? row_end - row_start : 0;
+  bool in_range = R <= 8 * (uint64_t)n + 4096;
+  for (size_t k = 0; k < n && in_range; ++k) in_range = v[k].a >= row_start && v[k].a < row_end;
+  if (!in_range) {
+    std::sort(v.begin(), v.end(), less);
+    return;
+  }
+  std::vector<uint32_t> pos((size_t)R + 1, 0);  // pos[r]: first slot of row r
+  for (const kg_pair& p : v) ++pos[(size_t)(p.a - row_start) + 1];
+  for (size_t r = 0; r < R; ++r) pos[r + 1] += pos[r];
+  std::vector<kg_pair> out(n);
+  unsigned nt = std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency()));
+  if (n < 20000) nt = 1;
+  // row blocks [rb[t], rb[t+1]) with about n / nt pairs each
+  std::vector<size_t> rb(nt + 1, (size_t)R);
+  rb[0] = 0;
+  for (unsigned t = 1; t < nt; ++t)
+    rb[t] = (size_t)(std::lower_bound(pos.begin(), pos.end(), (uint32_t)(n * t / nt)) - pos.begin());
+  for (unsigned t = 1; t < nt; ++t) rb[t] = std::min(std::max(rb[t], rb[t - 1]), (size_t)R);
+  auto work = [&](unsigned t) {
+    const size_t r0 = rb[t], r1 = rb[t + 1];
+    if (r0 >= r1) return;
+    std::vector<uint32_t> next(pos.begin() + (long)r0, pos.begin() + (long)r1);
+    for (const kg_pair& p : v) {
+      const size_t r = (size_t)(p.a - row_start);
+      if (r >= r0 && r < r1) out[next[r - r0]++] = p;  // stable within a row
+    }
+    for (size_t r = r0; r < r1; ++r) {
+      const size_t b0 = pos[r], b1 = pos[r + 1];
+      if (b1 - b0 <= 1) continue;
+      if (b1 - b0 <= 16) {
+        for (size_t k = b0 + 1; k < b1; ++k)  // insertion sort by b
+          for (size_t m = k; m > b0 && out[m].b < out[m - 1].b; --m) std::swap(out[m], out[m - 1]);
+      } else {
+        std::sort(out.begin() + (long)b0, out.begin() + (long)b1, less);
+      }
+    }
+  };
+  if (nt == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t) th.emplace_back(work, t);
+    for (auto& t : th) t.join();
+  }
+  v.swap(out);
 }
 
 }  // namespace
@@ -141,8 +200,7 @@ int kg_pairs_run_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t n_kmers, uint
   if (cnt[1])
     KG_CUDA(cudaMemcpy(ctx->pairs.data(), ctx->dPairs, cnt[1] * sizeof(kg_pair), cudaMemcpyDeviceToHost),
             "copy pairs");
-  std::sort(ctx->pairs.begin(), ctx->pairs.end(),
-            [](const kg_pair& x, const kg_pair& y) { return x.a != y.a ? x.a < y.a : x.b < y.b; });
+  sort_pairs(ctx->pairs, row_start, row_end);
   if (res) {
     res->n_evaluated = cnt[0];
     res->n_pairs = cnt[1];
