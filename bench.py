@@ -629,6 +629,95 @@ def run_sorted(args):
     api.lib().kg_host_free(hbuf)
 
 
+FILES = dict(n=1000, m=1_000_000, r=16, seed=50)
+
+
+def run_files(args):
+    """End to end through the programs, as the pipeline calls them: the
+    reference's kgwas and this package's bin/kgwas on the same files of one
+    batch (n=1000, r=16+1, 1M k-mers, CORR_THRESHOLD=0, files in the page
+    cache): COLS mode on the batch_*/ column files (first read, then with the
+    packed .kbits sidecar) and ROWS mode on a kmer<TAB>bitstring file.  Wall
+    clock of each process, one run each (a run is seconds long)."""
+    import subprocess
+    from supergwas_b200 import build, synth
+    from oracle import oracle as O
+    rank, world, local = rank_env()
+    if rank != 0:
+        return
+    build.build_all()
+    F = dict(FILES)
+    if args.kmers:
+        F["m"] = args.kmers
+    n, m, r = F["n"], F["m"], F["r"]
+    threads = os.cpu_count() or 1
+    env = {"CORR_THRESHOLD": "0", "LOAD_THREADS": str(threads), "BLAS_THREADS": str(threads),
+           "EMIT_THREADS": str(threads), "KGWAS_DEVICE": str(local)}
+    t_gen = time.perf_counter()
+    with tempfile.TemporaryDirectory() as d:
+        ds = synth.simulate(n=n, m=m, S=WORKLOAD["S"], r=r, n_causal=50, missing=WORKLOAD["missing"],
+                            seed=F["seed"], structure_kmers=min(50_000, m))
+        paths = synth.write_dataset(d, ds)
+        rows = os.path.join(d, "rows.tsv")
+        synth.write_rows_file(rows, ds.packed_all, ds.n_all, ds.kmers)
+        for root, _, files in os.walk(d):  # into the page cache
+            for f in files:
+                with open(os.path.join(root, f), "rb") as fh:
+                    while fh.read(1 << 24):
+                        pass
+        t_gen = time.perf_counter() - t_gen
+
+        def run(exe_args, extra, tag, reference=False):
+            out = os.path.join(d, tag, "batch_000.tsv")
+            os.makedirs(os.path.dirname(out), exist_ok=True)
+            e = dict(env, **extra)
+            t0 = time.perf_counter()
+            if reference:
+                res = O.run_reference([*exe_args[:4], out, "6", *exe_args[4:]], e)
+            else:
+                res = subprocess.run([build.CLI, *exe_args[:4], out, "6", *exe_args[4:]],
+                                     env=dict(os.environ, **e), capture_output=True, text=True)
+            dt = time.perf_counter() - t0
+            if res.returncode != 0:
+                raise RuntimeError(f"{tag}: {res.stderr[-500:]}")
+            count = open(out + ".count").read()
+            nrows = sum(1 for _ in open(out))
+            phases[tag] = [ln for ln in res.stderr.splitlines() if ln.startswith("[TIME]")]
+            return int(count.split("\t")[1]), dt, count, nrows
+
+        phases = {}
+        base = [paths["samples"], paths["pheno"]]
+        cols = [*base, paths["batch"], paths["ubin"], "--mode", "cols"]
+        rowsa = [*base, rows, paths["ubin"], "--mode", "rows"]
+        run(cols, {}, "warm")  # GPU context and library load once
+        t_c, s_c, c_c, h_c = run(cols, {}, "cols")
+        run(cols, {"KGWAS_KBITS": "1"}, "kb_write")
+        t_k, s_k, c_k, h_k = run(cols, {"KGWAS_KBITS": "1"}, "kb_read")
+        t_r, s_r, c_r, h_r = run(rowsa, {}, "rows")
+        t_rc, s_rc, c_rc, h_rc = run(cols, {}, "ref_cols", reference=True)
+        t_rr, s_rr, c_rr, h_rr = run(rowsa, {}, "ref_rows", reference=True)
+    same = c_c == c_k == c_rc and c_r == c_rr
+    line = {"metric": "k-mer tests/s end to end through the kgwas program (files in, files out)",
+            "value": t_c / s_c, "unit": "k-mer tests/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "ms_per_step": 1e3 * s_c, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "i8 limbs -> i32 TMEM, f64 epilogue", "data": "synthetic (seeded), written as pipeline files",
+            "config": {"workload": f"files: n={n} (5% unphenotyped), {m} k-mers in one batch_*/ directory "
+                                   f"({n} column files) and one ROWS file, r={r}+1, CORR_THRESHOLD=0, "
+                                   f"files in the page cache, {threads} host threads for both programs",
+                       "parallelism": "1 GPU + host threads"},
+            "e2e": {"value": t_c / s_c, "unit": "k-mer tests/s", "h2d_bytes_per_step": m * 128,
+                    "d2h_bytes_per_step": None},
+            "cols_seconds": s_c, "cols_kbits_seconds": s_k, "rows_seconds": s_r,
+            "cols_kbits": t_k / s_k, "rows": t_r / s_r,
+            "reference_cols": t_rc / s_rc, "reference_cols_seconds": s_rc,
+            "reference_rows": t_rr / s_rr, "reference_rows_seconds": s_rr,
+            "count_lines_identical": same, "emitted_rows": {"cols": h_c, "reference_cols": h_rc, "rows": h_r,
+                                                            "reference_rows": h_rr},
+            "phases": {k: v for k, v in phases.items() if k in ("cols", "kb_read", "rows")},
+            "gpu_launches": None, "gen_seconds": t_gen}
+    print(json.dumps(line), flush=True)
+
+
 PAIRS = dict(n=1000, N=50_000, S=8, r=16, seed=48, cpu_N=3000)
 
 
@@ -738,10 +827,11 @@ def main():
     ap.add_argument("--ref-kmers", type=int, default=250_000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="precision",
-                    choices=["precision", "batched", "streaming", "pairs", "sorted"],
+                    choices=["precision", "batched", "streaming", "pairs", "sorted", "files"],
                     help="precision: the default single-phenotype workload; batched: 64 phenotypes; "
                          "streaming: 8 phenotypes at n=5000 from pinned host memory; pairs: the 2-D pair test; "
-                         "sorted: end to end on a batch with runs of equal rows")
+                         "sorted: end to end on a batch with runs of equal rows; "
+                         "files: the kgwas program against the reference's on the same files")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours" and not os.environ.get("KG_BENCH_ALLOW_SHORT"):
         args.warmup = 3
@@ -755,6 +845,8 @@ def main():
         run_pairs(args)
     elif args.workload == "sorted":
         run_sorted(args)
+    elif args.workload == "files":
+        run_files(args)
     else:
         run_ours(args)
 

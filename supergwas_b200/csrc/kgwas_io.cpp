@@ -17,15 +17,23 @@
 #include <fstream>
 #include <iostream>
 #include <memory>
+#include <mutex>
 #include <sstream>
 
 #include <omp.h>
 
 namespace kgio {
 
+// One [ERROR] line even when several threads fail at once, and no exit-time
+// teardown while another thread may be inside the CUDA runtime (the programs
+// set up the GPU on a thread of their own while they read their inputs).
 void die(const std::string& m) {
+  static std::mutex mu;
+  mu.lock();
   std::cerr << "[ERROR] " << m << "\n";
-  std::exit(1);
+  std::cerr.flush();
+  std::fflush(stdout);
+  std::_Exit(1);
 }
 
 void warn(const std::string& m) { std::cerr << "[WARN] " << m << "\n"; }
@@ -346,79 +354,182 @@ void load_matrix_packed(const std::string& bits_dir, const std::vector<int>& idx
 }
 
 // ------------------------------------------------------------ ROWS reader
-RowsReader::RowsReader(const std::string& path) {
+RowsReader::RowsReader(const std::string& path, int nthreads) : threads(std::max(1, nthreads)) {
   const bool gzm = path.size() >= 3 && path.compare(path.size() - 3, 3, ".gz") == 0;
   if (gzm) {
     gzFile f = gzopen(path.c_str(), "rb");
     if (!f) die("Cannot open gz file: " + path);
     gzbuffer(f, 1u << 20);
     gz = f;
+    buf.resize((size_t)64 << 20);
   } else {
-    auto* in = new std::ifstream(path);
-    if (!*in) {
-      delete in;
+    const int fd = ::open(path.c_str(), O_RDONLY);
+    if (fd < 0) die("Cannot open kmer file: " + path);
+    struct stat st {};
+    if (fstat(fd, &st) != 0) {
+      ::close(fd);
       die("Cannot open kmer file: " + path);
     }
-    plain = in;
+    map_sz = (size_t)st.st_size;
+    if (map_sz > 0) {
+      void* p = mmap(nullptr, map_sz, PROT_READ, MAP_PRIVATE, fd, 0);
+      if (p == MAP_FAILED) {
+        ::close(fd);
+        die("mmap: " + path);
+      }
+      madvise(p, map_sz, MADV_SEQUENTIAL);
+      map = (const char*)p;
+    }
+    ::close(fd);
+    end = map_sz;
+    eof = true;
   }
 }
 
 RowsReader::~RowsReader() {
   if (gz) gzclose((gzFile)gz);
-  delete (std::ifstream*)plain;
+  if (map) munmap((void*)map, map_sz);
 }
 
-// src/kgwas.cpp:318-341 for gz input (drops one '\r' before '\n'),
-// std::getline for plain input.
-bool RowsReader::next_line(std::string& out) {
-  if (plain) return (bool)std::getline(*(std::ifstream*)plain, out);
-  out.clear();
-  static thread_local std::unique_ptr<char[]> buf(new char[1u << 20]);
-  bool got_any = false;
-  for (;;) {
-    char* res = gzgets((gzFile)gz, buf.get(), (int)(1u << 20));
-    if (!res) return got_any;
-    got_any = true;
-    size_t len = std::strlen(res);
-    if (len == 0) continue;
-    if (res[len - 1] == '\n') {
-      size_t end = len - 1;
-      if (end > 0 && res[end - 1] == '\r') --end;
-      out.append(res, res + end);
-      return true;
-    }
-    out.append(res, res + len);
+// gz input: appends inflated bytes after [beg, end), moving the unparsed rest
+// to the front first and growing the buffer when one line fills it; sets eof
+// at the end of the stream.
+void RowsReader::fill() {
+  if (map) return;
+  if (beg > 0) {
+    std::memmove(buf.data(), buf.data() + beg, end - beg);
+    end -= beg;
+    beg = 0;
   }
+  if (end == buf.size()) buf.resize(2 * buf.size());
+  const int r = gzread((gzFile)gz, buf.data() + end, (unsigned)std::min<size_t>(buf.size() - end, 1u << 30));
+  if (r < 0) {
+    int err = 0;
+    const char* msg = gzerror((gzFile)gz, &err);
+    die(std::string("gzread error: ") + (msg ? msg : ""));
+  }
+  if (r == 0) eof = true;
+  end += (size_t)r;
 }
 
+// src/kgwas.cpp:435-459.  Lines as the reference reads them: std::getline for
+// plain input (a '\r' stays in the line), gzgets for gz input with one '\r'
+// before '\n' dropped (:318-341); empty lines skipped; the k-mer ends at the
+// first tab, else the first space, else the line is skipped; overlap sample j
+// is character idxs[j] of the bitstring (one past its end reads '\0').
 size_t RowsReader::read(size_t max_rows, const std::vector<int>& idxs, std::vector<std::string>& kmers,
                         std::vector<uint64_t>& packed) {
   const int n = (int)idxs.size();
   const uint32_t W = words_per_kmer(n);
-  std::string line;
   size_t got = 0;
-  while (got < max_rows && next_line(line)) {
-    if (line.empty()) continue;
-    ++lines;
-    size_t tab = line.find('\t');
-    if (tab == std::string::npos) {
-      tab = line.find(' ');
-      if (tab == std::string::npos) continue;
+  std::vector<size_t> ls, le;  // line spans [ls, le) of this round
+  std::vector<size_t> sep;     // separator position (or SIZE_MAX: no row)
+  std::vector<size_t> slot;    // output row of each line
+  while (got < max_rows) {
+    ls.clear();
+    le.clear();
+    const size_t want = max_rows - got;
+    const char* B0 = data();
+    // line ends in a window of up to 256 MB, found by the threads in equal
+    // pieces and kept in file order
+    const size_t win = std::min(end - beg, (size_t)256 << 20);
+    const unsigned nt = win >= ((size_t)4 << 20) ? (unsigned)threads : 1u;
+    std::vector<std::vector<size_t>> nls(nt);
+#pragma omp parallel for num_threads(nt) schedule(static, 1)
+    for (int t = 0; t < (int)nt; ++t) {
+      const size_t a = beg + win * (size_t)t / nt, b = beg + win * (size_t)(t + 1) / nt;
+      for (size_t q = a; q < b;) {
+        const char* nl = (const char*)std::memchr(B0 + q, '\n', b - q);
+        if (!nl) break;
+        nls[t].push_back((size_t)(nl - B0));
+        q = nls[t].back() + 1;
+      }
     }
-    const size_t nb = line.size() - (tab + 1);
-    const char* bits = line.data() + tab + 1;
-    const size_t base = packed.size();
-    packed.resize(base + W, 0ull);
-    for (int j = 0; j < n; ++j) {
-      const size_t pos = (size_t)idxs[j];
-      char c;
-      if (pos < nb) c = bits[pos];
-      else if (pos == nb) c = '\0';  // std::string::operator[] at size()
-      else die("bitstring shorter than the samples list in row: " + line.substr(0, tab));
-      if (c == '1') packed[base + (size_t)(j >> 6)] |= 1ull << (j & 63);
+    size_t p = beg;
+    for (unsigned t = 0; t < nt && ls.size() < want; ++t)
+      for (size_t e : nls[t]) {
+        if (ls.size() >= want) break;
+        ls.push_back(p);
+        le.push_back(e);
+        p = e + 1;
+      }
+    if (ls.empty() && win < end - beg) {  // a line longer than the window
+      const char* nl = (const char*)std::memchr(B0 + beg, '\n', end - beg);
+      if (nl) {
+        ls.push_back(beg);
+        le.push_back((size_t)(nl - B0));
+        p = le.back() + 1;
+      }
     }
-    kmers.emplace_back(line, 0, tab);
-    ++got;
+    if (ls.empty()) {
+      if (!eof) {
+        fill();
+        continue;
+      }
+      if (beg == end) break;
+      ls.push_back(beg);  // a last line without '\n'
+      le.push_back(end);
+      p = end;
+    }
+    beg = p;
+    const size_t L = ls.size();
+    sep.assign(L, SIZE_MAX);
+    slot.assign(L, 0);
+    const char* B = data();
+    // pass 1: which lines are rows, and where their k-mers end
+    size_t nonempty = 0;
+#pragma omp parallel for num_threads(threads) schedule(static) reduction(+ : nonempty)
+    for (int64_t t = 0; t < (int64_t)L; ++t) {
+      size_t e = le[t];
+      if (gz && e > ls[t] && B[e - 1] == '\r') le[t] = --e;
+      if (e == ls[t]) continue;
+      ++nonempty;
+      const char* a = B + ls[t];
+      const void* tb = std::memchr(a, '\t', e - ls[t]);
+      if (!tb) tb = std::memchr(a, ' ', e - ls[t]);
+      if (tb) sep[t] = (size_t)((const char*)tb - B);
+    }
+    lines += nonempty;
+    size_t rows = 0;
+    for (size_t t = 0; t < L; ++t) {
+      slot[t] = rows;
+      rows += sep[t] != SIZE_MAX ? 1 : 0;
+    }
+    const size_t k0 = kmers.size(), p0 = packed.size();
+    kmers.resize(k0 + rows);
+    packed.resize(p0 + rows * W, 0ull);
+    // pass 2: pack the rows; the first row (in file order) whose bitstring is
+    // too short is the error
+    std::atomic<size_t> bad{SIZE_MAX};
+#pragma omp parallel for num_threads(threads) schedule(static)
+    for (int64_t t = 0; t < (int64_t)L; ++t) {
+      if (sep[t] == SIZE_MAX) continue;
+      const char* bits = B + sep[t] + 1;
+      const size_t nb = le[t] - (sep[t] + 1);
+      uint64_t* row = packed.data() + p0 + slot[t] * W;
+      bool ok = true;
+      for (int j = 0; j < n; ++j) {
+        const size_t pos = (size_t)idxs[j];
+        if (pos < nb) {
+          if (bits[pos] == '1') row[j >> 6] |= 1ull << (j & 63);
+        } else if (pos > nb) {
+          ok = false;
+          break;
+        }
+      }
+      if (!ok) {
+        size_t cur = bad.load();
+        while ((size_t)t < cur && !bad.compare_exchange_weak(cur, (size_t)t)) {
+        }
+        continue;
+      }
+      kmers[k0 + slot[t]].assign(B + ls[t], sep[t] - ls[t]);
+    }
+    if (bad.load() != SIZE_MAX) {
+      const size_t t = bad.load();
+      die("bitstring shorter than the samples list in row: " + std::string(B + ls[t], sep[t] - ls[t]));
+    }
+    got += rows;
   }
   return got;
 }

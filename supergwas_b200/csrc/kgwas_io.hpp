@@ -55,8 +55,10 @@ void load_matrix_packed(const std::string& bits_dir, const std::vector<int>& idx
 
 // ROWS-mode input (src/kgwas.cpp:435-459): "kmer<TAB or SPACE>bitstring" lines,
 // x_j = (bits[idxs[j]] == '1').  Appends to kmers/packed.
+// Lines are parsed in parallel (`threads` host threads) from large blocks of
+// the file; the rows come back in file order.
 struct RowsReader {
-  explicit RowsReader(const std::string& path);
+  explicit RowsReader(const std::string& path, int threads = 1);
   ~RowsReader();
   // Reads up to max_rows rows; returns the number read (0 at end).
   size_t read(size_t max_rows, const std::vector<int>& idxs, std::vector<std::string>& kmers,
@@ -64,8 +66,14 @@ struct RowsReader {
   size_t lines = 0;   // non-empty lines seen (the reference's line_count)
  private:
   void* gz = nullptr;
-  void* plain = nullptr;
-  bool next_line(std::string& line);
+  const char* map = nullptr;  // a plain file, mapped whole
+  size_t map_sz = 0;
+  int threads = 1;
+  std::vector<char> buf;  // gz: inflated bytes [beg, end) not yet parsed
+  size_t beg = 0, end = 0;
+  bool eof = false;
+  const char* data() const { return map ? map : buf.data(); }
+  void fill();
 };
 
 // Sharded k-mer index with bitstrings (the input of the 2-D pair test):

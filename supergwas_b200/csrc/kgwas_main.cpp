@@ -25,6 +25,8 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <memory>
+#include <thread>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -132,40 +134,46 @@ static Config parse_args(int argc, char** argv) {  // src/kgwas.cpp:67-126
 }
 
 // ------------------------------------------------------------- GPU context
+// The context is created on a thread of its own (start) while the program
+// reads its inputs; open() waits for it and reports a failure at the point
+// where the reference would meet it, after the inputs.
 struct Gpu {
   kg_ctx* ctx = nullptr;
-  ~Gpu() { kg_destroy(ctx); }
-  void check(int rc, const char* what) {
-    if (rc != KG_OK) die(string("GPU ") + what + " failed (code " + std::to_string(rc) + "): " + kg_last_error(ctx));
+  std::thread th;
+  int rc = KG_OK;
+  ~Gpu() {
+    if (th.joinable()) th.join();
+    kg_destroy(ctx);
   }
-  void open(const Config& cfg) {
+  void check(int rc_, const char* what) {
+    if (rc_ != KG_OK) die(string("GPU ") + what + " failed (code " + std::to_string(rc_) + "): " + kg_last_error(ctx));
+  }
+  void start(const Config& cfg) {
     kg_opts o;
     kg_default_opts(&o);
     o.device = cfg.device;
     o.precision = cfg.precision;
     o.corr_threshold = cfg.corr_threshold;
     o.log10_thresh = cfg.log10_thresh;
-    const int rc = kg_create(&ctx, &o);
+    th = std::thread([this, o] { rc = kg_create(&ctx, &o); });
+  }
+  void open(const Config& cfg) {
+    if (!th.joinable() && !ctx) start(cfg);
+    if (th.joinable()) th.join();
     if (rc != KG_OK) die("GPU context creation failed (code " + std::to_string(rc) + ") on device " +
                          std::to_string(cfg.device));
   }
 };
 
-// Pinned host buffer for the packed matrix (pageable fallback).
+// Host buffer for the packed matrix.  Pageable: no CUDA call is needed before
+// the inputs are read, and kg_run_host stages pageable rows through its own
+// pinned buffers (where it also finds runs of equal rows).
 struct HostWords {
   uint64_t* p = nullptr;
-  bool pinned = false;
-  vector<uint64_t> v;
+  std::unique_ptr<uint64_t[]> v;
   void alloc(size_t words) {
-    p = (uint64_t*)kg_host_alloc(words * 8);
-    pinned = p != nullptr;
-    if (!p) {
-      v.assign(words, 0);
-      p = v.data();
-    }
-  }
-  ~HostWords() {
-    if (pinned) kg_host_free(p);
+    v.reset(new uint64_t[words ? words : 1]);  // every word is written by the reader
+    p = v.get();
   }
 };
 
@@ -319,13 +327,17 @@ static void kbits_write(const string& path, size_t N, int n, uint32_t W, uint64_
 
 static void run_cols(const Config& cfg) {  // src/kgwas.cpp:168-307
   kgio::Timer tall;
+  Gpu g;
+  g.start(cfg);
   kgio::Overlap ov = kgio::build_overlap(cfg.samples_file, cfg.pheno_file);
   const int n = (int)ov.y.size();
   kgio::UData ud = kgio::load_ubin(cfg.U_file, n);
   const string bits_dir = cfg.input_path + "/bits";
   const string kmers_gz = cfg.input_path + "/kmers.txt.gz";
   const size_t N = kgio::infer_N_from_bits(bits_dir, ov.idxs.front());
-  vector<string> kmers = kgio::load_kmers(kmers_gz, N);
+  // the k-mer strings are read beside the columns
+  vector<string> kmers;
+  std::thread kt([&] { kmers = kgio::load_kmers(kmers_gz, N); });
   const uint32_t W = kgio::words_per_kmer(n);
   HostWords X;
   X.alloc((size_t)N * W);
@@ -339,8 +351,9 @@ static void run_cols(const Config& cfg) {  // src/kgwas.cpp:168-307
     kgio::load_matrix_packed(bits_dir, ov.idxs, N, cfg.LOAD_THREADS, X.p);
     if (use_kbits) kbits_write(kpath, N, n, W, h, X.p);
   }
+  kt.join();
+  std::cerr << "[TIME] inputs read " << tall.sec() << " s\n";
 
-  Gpu g;
   g.open(cfg);
   kgio::Timer tg;
   double yyM = 0;
@@ -385,6 +398,8 @@ static void run_cols(const Config& cfg) {  // src/kgwas.cpp:168-307
 
 static void run_rows(const Config& cfg) {  // src/kgwas.cpp:343-522
   kgio::Timer tall;
+  Gpu g;
+  g.start(cfg);
   const auto all_ids = kgio::load_lines(cfg.samples_file);
   const auto pheno = kgio::load_pheno(cfg.pheno_file);
   vector<int> idxs;
@@ -410,7 +425,7 @@ static void run_rows(const Config& cfg) {  // src/kgwas.cpp:343-522
   uin.read((char*)U.data(), (std::streamsize)(sizeof(double) * (size_t)n * r));
   std::cerr << "[INFO] CORR_THRESHOLD=" << cfg.corr_threshold << "\n";
 
-  kgio::RowsReader rr(cfg.input_path);
+  kgio::RowsReader rr(cfg.input_path, cfg.LOAD_THREADS);
   std::ofstream out(cfg.out_file);
   if (!out) die("Cannot open output: " + cfg.out_file);
   const bool do_2d = (cfg.log10_thresh_2d > 0.0);
@@ -422,11 +437,6 @@ static void run_rows(const Config& cfg) {  // src/kgwas.cpp:343-522
     out2d.open(p2);
     if (!out2d) die("Cannot open 2D output: " + p2);
   }
-  Gpu g;
-  g.open(cfg);
-  double yyM = 0;
-  g.check(kg_set_structure(g.ctx, U.data(), n, r, y.data(), &yyM), "set_structure");
-  if (!(yyM > 1e-12)) std::cerr << "[WARN] yyM ~ 0. Tests unstable.\n";
   const uint32_t W = kgio::words_per_kmer(n);
   uint64_t passed = 0;
   const size_t BATCH = (size_t)1 << 22;
@@ -434,13 +444,21 @@ static void run_rows(const Config& cfg) {  // src/kgwas.cpp:343-522
   vector<uint64_t> packed;
   vector<kgio::IndexRow> index1, index2;
   string first_kmer;
-  for (;;) {
-    kmers.clear();
-    packed.clear();
-    const size_t got = rr.read(BATCH, idxs, kmers, packed);
-    if (got == 0) break;
+  double t_read = 0, t_gpu = 0;
+  // the first batch is read while the GPU context is set up
+  kgio::Timer tr;
+  size_t got = rr.read(BATCH, idxs, kmers, packed);
+  t_read += tr.sec();
+  g.open(cfg);
+  double yyM = 0;
+  g.check(kg_set_structure(g.ctx, U.data(), n, r, y.data(), &yyM), "set_structure");
+  if (!(yyM > 1e-12)) std::cerr << "[WARN] yyM ~ 0. Tests unstable.\n";
+  for (; got > 0; kmers.clear(), packed.clear(), tr = kgio::Timer(), got = rr.read(BATCH, idxs, kmers, packed),
+                  t_read += tr.sec()) {
     kg_result res{};
+    kgio::Timer tg;
     g.check(kg_run_host(g.ctx, packed.data(), got, W, &res, nullptr), "run");
+    t_gpu += tg.sec();
     passed += res.n_tested;
     string one, two;
     format_hits(res, kmers, packed.data(), W, n, do_2d, p_thresh_2d, one, two,
@@ -457,6 +475,7 @@ static void run_rows(const Config& cfg) {  // src/kgwas.cpp:343-522
   out.close();
   write_indexes(cfg, vector<string>{first_kmer}, index1, index2);
   write_count(cfg.out_file, passed);
+  std::cerr << "[TIME] rows read " << t_read << " s, GPU tests " << t_gpu << " s\n";
   std::cerr << "[TIME] End-to-end " << tall.sec() << "s\n";
 }
 

@@ -4,6 +4,7 @@ import json
 import os
 import shutil
 import subprocess
+import sys
 import tempfile
 
 import numpy as np
@@ -313,4 +314,118 @@ def test_run_finder(built, m, wpk, s0, cnt):
     assert np.array_equal(first[:nu], exp_first)
     assert np.array_equal(lens[:nu], exp_len)
     assert np.array_equal(out[:nu], X[exp_first])
+
+
+def _rows_lib():
+    out = os.path.join(HERE, "native", "_build", "librows_check.so")
+    src = [os.path.join(HERE, "native", "rows_check.cpp"), os.path.join(build.CSRC, "kgwas_io.cpp")]
+    deps = src + [os.path.join(build.CSRC, "kgwas_io.hpp")]
+    if not os.path.exists(out) or any(os.path.getmtime(d) > os.path.getmtime(out) for d in deps):
+        os.makedirs(os.path.dirname(out), exist_ok=True)
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", out, *src, "-lz"],
+                       check=True)
+    L = ctypes.CDLL(out)
+    vp = ctypes.c_void_p
+    L.rows_parse.argtypes = [ctypes.c_char_p, vp, ctypes.c_int, ctypes.c_int, ctypes.c_ulong, vp, ctypes.c_ulong,
+                             vp, ctypes.c_ulong, vp, vp]
+    L.rows_parse.restype = ctypes.c_long
+    return L
+
+
+def _rows_expected(lines, idxs, gz):
+    """src/kgwas.cpp:435-459 restated: the rows, k-mers and non-empty lines of a ROWS file."""
+    n = len(idxs)
+    W = synth.words_per_kmer(n)
+    kmers, rows, nonempty = [], [], 0
+    for ln in lines:
+        if gz and ln.endswith("\r"):
+            ln = ln[:-1]
+        if not ln:
+            continue
+        nonempty += 1
+        t = ln.find("\t")
+        if t < 0:
+            t = ln.find(" ")
+        if t < 0:
+            continue
+        bits = ln[t + 1:]
+        row = np.zeros(W, np.uint64)
+        for j, pos in enumerate(idxs):
+            assert pos <= len(bits)
+            if pos < len(bits) and bits[pos] == "1":
+                row[j >> 6] |= np.uint64(1 << (j & 63))
+        kmers.append(ln[:t])
+        rows.append(row)
+    return kmers, np.array(rows, np.uint64).reshape(-1, W), nonempty
+
+
+@pytest.mark.parametrize("gz", [False, True])
+@pytest.mark.parametrize("threads,max_rows", [(1, 10**6), (8, 10**6), (8, 7), (3, 1)])
+def test_rows_reader(tmp_path, gz, threads, max_rows):
+    """The parallel ROWS reader gives the rows of the line-by-line reading of
+    src/kgwas.cpp:435-459: tab or space separators, lines without one skipped,
+    empty lines, '\\r' (kept in plain files, dropped before '\\n' in gz
+    files), a bitstring one character short reading '\\0', a last line without
+    '\\n', in batches of at most max_rows rows."""
+    import gzip
+    rng = np.random.default_rng(threads * 31 + max_rows + gz)
+    n_all = 150
+    idxs = sorted(rng.choice(n_all, size=120, replace=False).tolist())
+    lines = []
+    for i in range(400):
+        k = "".join(rng.choice(list("ACGT"), size=31))
+        bits = "".join(rng.choice(["0", "1"], size=n_all))
+        kind = i % 9
+        if kind == 1:
+            lines.append("")
+        elif kind == 2:
+            lines.append(k + " " + bits)
+        elif kind == 3:
+            lines.append(k + "_noseparator")
+        elif kind == 4:
+            lines.append(k + "\t" + bits + "\r")
+        elif kind == 5:
+            lines.append(k + "\t" + bits[: idxs[-1]])      # one short: reads the terminator
+        else:
+            lines.append(k + "\t" + bits)
+    text = "\n".join(lines)                                 # no '\\n' after the last line
+    path = tmp_path / ("rows.tsv.gz" if gz else "rows.tsv")
+    if gz:
+        with gzip.open(path, "wb") as f:
+            f.write(text.encode())
+    else:
+        path.write_text(text)
+    exp_k, exp_rows, exp_lines = _rows_expected(lines, idxs, gz)
+    L = _rows_lib()
+    W = synth.words_per_kmer(len(idxs))
+    packed = np.zeros(len(lines) * W, np.uint64)
+    kbuf = ctypes.create_string_buffer(len(text) + 16)
+    nl, nb = ctypes.c_ulong(0), ctypes.c_ulong(0)
+    ia = np.array(idxs, np.int32)
+    got = L.rows_parse(str(path).encode(), ia.ctypes.data, len(idxs), threads, max_rows, packed.ctypes.data,
+                       packed.size, ctypes.addressof(kbuf), len(kbuf), ctypes.byref(nl), ctypes.byref(nb))
+    assert got == len(exp_k)
+    assert kbuf.value.decode().split("\n")[:-1] == exp_k
+    assert np.array_equal(packed[: got * W].reshape(-1, W), exp_rows)
+    assert nl.value == exp_lines
+    assert nb.value == (got + max_rows - 1) // max_rows if max_rows < got else nb.value == 1
+
+
+def test_rows_reader_short_bitstring(tmp_path):
+    """A bitstring that ends before an overlap sample's position stops the
+    program with the first such row's k-mer, in file order."""
+    p = tmp_path / "rows.tsv"
+    p.write_text("AAA\t0101\nCCC\t01\nGGG\t0\n")
+    _rows_lib()  # built here; the child process only loads it
+    lib = os.path.join(HERE, "native", "_build", "librows_check.so")
+    code = ("import ctypes, numpy as np; L = ctypes.CDLL(%r); vp = ctypes.c_void_p; "
+            "L.rows_parse.argtypes = [ctypes.c_char_p, vp, ctypes.c_int, ctypes.c_int, ctypes.c_ulong, vp, "
+            "ctypes.c_ulong, vp, ctypes.c_ulong, vp, vp]; "
+            "ia = np.array([0, 3], np.int32); b = np.zeros(64, np.uint64); k = ctypes.create_string_buffer(256); "
+            "n = ctypes.c_ulong(); m = ctypes.c_ulong(); "
+            "L.rows_parse(%r, ia.ctypes.data, 2, 4, 100, b.ctypes.data, 64, ctypes.addressof(k), 256, "
+            "ctypes.byref(n), ctypes.byref(m))") % (lib, str(p).encode())
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=HERE)
+    assert r.returncode == 1
+    assert r.stderr.strip().splitlines()[-1] == "[ERROR] bitstring shorter than the samples list in row: CCC"
 
