@@ -19,6 +19,7 @@
 #include <iostream>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/kgwas_cuda.h"
@@ -69,17 +70,40 @@ static Config parse_args(int argc, char** argv) {  // src/kgwas_2d.cpp:45-78
   return cfg;
 }
 
+// The context is created on a thread of its own while the index is read;
+// a failure is reported where the reference would meet it, after the inputs.
 struct Gpu {
   kg_ctx* ctx = nullptr;
-  ~Gpu() { kg_destroy(ctx); }
-  void check(int rc, const char* what) {
-    if (rc != KG_OK) die(string("GPU ") + what + " failed (code " + std::to_string(rc) + "): " + kg_last_error(ctx));
+  std::thread th;
+  int rc = KG_OK;
+  ~Gpu() {
+    if (th.joinable()) th.join();
+    kg_destroy(ctx);
+  }
+  void check(int rc_, const char* what) {
+    if (rc_ != KG_OK) die(string("GPU ") + what + " failed (code " + std::to_string(rc_) + "): " + kg_last_error(ctx));
+  }
+  void start(const kg_opts& o) {
+    th = std::thread([this, o] { rc = kg_create(&ctx, &o); });
+  }
+  void wait(int device) {
+    if (th.joinable()) th.join();
+    if (rc != KG_OK) die("GPU context creation failed (code " + std::to_string(rc) + ") on device " +
+                         std::to_string(device));
   }
 };
 
 int main(int argc, char** argv) {
   const Config cfg = parse_args(argc, argv);
   kgio::Timer tall;
+  Gpu g;
+  {
+    kg_opts o;
+    kg_default_opts(&o);
+    o.device = cfg.device;
+    o.log10_thresh = cfg.log10_thresh;
+    g.start(o);
+  }
   const kgio::Overlap ov = kgio::build_overlap(cfg.samples_file, cfg.pheno_file);
   const int n = (int)ov.y.size();
   const kgio::UData ud = kgio::load_ubin(cfg.U_file, n);
@@ -117,14 +141,7 @@ int main(int argc, char** argv) {
   // GPU is touched so that the failure needs no device
   if (N < 2) die("emit_pairs_self: need at least 2 columns");
   // build_stats2d_self + emit_pairs_self (src/kgwas_2d.cpp:210-392) on the GPU
-  Gpu g;
-  kg_opts o;
-  kg_default_opts(&o);
-  o.device = cfg.device;
-  o.log10_thresh = cfg.log10_thresh;
-  const int rc = kg_create(&g.ctx, &o);
-  if (rc != KG_OK) die("GPU context creation failed (code " + std::to_string(rc) + ") on device " +
-                       std::to_string(cfg.device));
+  g.wait(cfg.device);
   double yyM = 0;
   g.check(kg_set_structure(g.ctx, ud.U.data(), n, ud.k, ov.y.data(), &yyM), "set_structure");
   if (!(yyM > 1e-12)) kgio::warn("yyM ~ 0");
