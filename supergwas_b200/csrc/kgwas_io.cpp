@@ -206,29 +206,39 @@ std::vector<std::string> load_kmers(const std::string& path, size_t N) {
   if (gz) {
     gzFile f = gzopen(path.c_str(), "rb");
     if (!f) die("gzopen: " + path);
-    const int BUFSZ = 1 << 15;
-    std::unique_ptr<char[]> buf(new char[BUFSZ]);
-    std::string line;
+    gzbuffer(f, 1u << 20);
+    // inflated in 4 MB blocks and split at '\n'; only '\n'-terminated lines
+    // count (an unterminated last line is not a k-mer), as with gzgets
+    std::vector<char> buf((size_t)4 << 20);
+    std::string part;  // a line that continues in the next block
     while (kmers.size() < N) {
-      char* r = gzgets(f, buf.get(), BUFSZ);
-      if (!r) {
+      const int r = gzread(f, buf.data(), (unsigned)buf.size());
+      if (r <= 0) {
         int err = 0;
         const char* msg = gzerror(f, &err);
-        if (err == Z_STREAM_END) break;
-        if (err != Z_OK) {
+        if (r < 0 || (err != Z_OK && err != Z_STREAM_END)) {
+          const std::string m = msg ? msg : "";
           gzclose(f);
-          die(std::string("gzgets error: ") + (msg ? msg : ""));
+          die("gzgets error: " + m);
         }
         break;
       }
-      char* nl = strchr(r, '\n');
-      if (nl) {
-        *nl = '\0';
-        line.append(r);
-        kmers.push_back(std::move(line));
-        line.clear();
-      } else {
-        line.append(r);
+      const char* p = buf.data();
+      const char* e = p + r;
+      while (p < e && kmers.size() < N) {
+        const char* nl = (const char*)std::memchr(p, '\n', (size_t)(e - p));
+        if (!nl) {
+          part.append(p, (size_t)(e - p));
+          break;
+        }
+        if (part.empty()) {
+          kmers.emplace_back(p, (size_t)(nl - p));
+        } else {
+          part.append(p, (size_t)(nl - p));
+          kmers.push_back(std::move(part));
+          part.clear();
+        }
+        p = nl + 1;
       }
     }
     gzclose(f);
