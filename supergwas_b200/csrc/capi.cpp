@@ -272,7 +272,6 @@ bool use_runs(const uint64_t* x, uint64_t m, uint32_t wpk, bool pageable) {
   if ((v && std::string(v) == "0") || m < 2 || m >= (1ull << 32)) return false;
   if (v && std::string(v) == "1") return true;
   if (!pageable || m < 4096) return false;
-  const size_t row = (size_t)wpk * 8;
   int dups = 0;
   for (int i = 0; i < 4096; ++i) {
     const uint64_t j = 1 + (uint64_t)i * (m - 1) / 4096;
@@ -332,8 +331,6 @@ bool find_runs(kg_ctx* ctx, const uint64_t* x, uint64_t m, uint32_t wpk, const s
   if (!use_runs(x, m, wpk, pageable)) return false;
   const char* v = std::getenv("KG_DEDUP");
   const bool force = v && std::string(v) == "1";
-  const size_t row = (size_t)wpk * 8;
-  (void)row;
   auto same = [&](uint64_t i) { return rows_equal(x + i * wpk, x + (i - 1) * wpk, wpk); };
   unsigned nt = std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency()));
   if (m < (1u << 16)) nt = 1;
