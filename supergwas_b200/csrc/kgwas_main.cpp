@@ -16,6 +16,8 @@
 //   --index-2d-out DIR  the same for the .2d rows (the .2d.tsv file; 4 shards
 //                       by default, as build_index_2d.sh), the input of kgwas_2d
 //                       (bin/kgwas_index_merge joins the indexes of batches)
+//   KGWAS_ROWS_BATCH rows per batch in ROWS mode (default 4194304); the next
+//                    batch is read while the current one is tested
 //   KGWAS_KBITS      1: keep the packed rows of the batch in a sidecar file
 //                    <batch>/kgwas_<N>_<n>_<hash>.kbits (hash of the overlap
 //                    sample positions) and reuse it instead of re-reading the
@@ -439,33 +441,51 @@ static void run_rows(const Config& cfg) {  // src/kgwas.cpp:343-522
   }
   const uint32_t W = kgio::words_per_kmer(n);
   uint64_t passed = 0;
-  const size_t BATCH = (size_t)1 << 22;
-  vector<string> kmers;
-  vector<uint64_t> packed;
+  size_t BATCH = (size_t)1 << 22;
+  if (const char* v = std::getenv("KGWAS_ROWS_BATCH")) BATCH = (size_t)std::max(1L, std::atol(v));
+  struct Batch {
+    vector<string> kmers;
+    vector<uint64_t> packed;
+    size_t got = 0;
+  } cur, nxt;
+  auto read_into = [&](Batch& b) {
+    b.kmers.clear();
+    b.packed.clear();
+    b.got = rr.read(BATCH, idxs, b.kmers, b.packed);
+  };
   vector<kgio::IndexRow> index1, index2;
   string first_kmer;
   double t_read = 0, t_gpu = 0;
-  // the first batch is read while the GPU context is set up
+  // the first batch is read while the GPU context is set up, and each next
+  // batch while the current one is tested and written
   kgio::Timer tr;
-  size_t got = rr.read(BATCH, idxs, kmers, packed);
+  read_into(cur);
   t_read += tr.sec();
   g.open(cfg);
   double yyM = 0;
   g.check(kg_set_structure(g.ctx, U.data(), n, r, y.data(), &yyM), "set_structure");
   if (!(yyM > 1e-12)) std::cerr << "[WARN] yyM ~ 0. Tests unstable.\n";
-  for (; got > 0; kmers.clear(), packed.clear(), tr = kgio::Timer(), got = rr.read(BATCH, idxs, kmers, packed),
-                  t_read += tr.sec()) {
+  while (cur.got > 0) {
+    double t_next = 0;
+    std::thread rd([&] {
+      kgio::Timer t;
+      read_into(nxt);
+      t_next = t.sec();
+    });
     kg_result res{};
     kgio::Timer tg;
-    g.check(kg_run_host(g.ctx, packed.data(), got, W, &res, nullptr), "run");
+    g.check(kg_run_host(g.ctx, cur.packed.data(), cur.got, W, &res, nullptr), "run");
     t_gpu += tg.sec();
     passed += res.n_tested;
     string one, two;
-    format_hits(res, kmers, packed.data(), W, n, do_2d, p_thresh_2d, one, two,
+    format_hits(res, cur.kmers, cur.packed.data(), W, n, do_2d, p_thresh_2d, one, two,
                 cfg.index_out.empty() ? nullptr : &index1, cfg.index_2d_out.empty() ? nullptr : &index2);
-    if (first_kmer.empty() && !kmers.empty()) first_kmer = kmers[0];
+    if (first_kmer.empty() && !cur.kmers.empty()) first_kmer = cur.kmers[0];
     out.write(one.data(), (std::streamsize)one.size());
     if (do_2d) out2d.write(two.data(), (std::streamsize)two.size());
+    rd.join();
+    t_read += t_next;
+    std::swap(cur, nxt);
   }
   std::cerr << "[INFO] Total kmers: " << rr.lines << ", passed correlation filter: " << passed << "\n";
   if (do_2d) {

@@ -138,3 +138,23 @@ def test_index_out_matches_build_index(built, mode):
     H.same_dir_files(idx1, os.path.join(work, "ref1"))
     H.same_dir_files(idx2, os.path.join(work, "ref2"))
     shutil.rmtree(work)
+
+
+def test_rows_batches_give_the_same_files(built):
+    """ROWS mode in batches of 37 rows (each next batch read while the current
+    one is tested) writes the same .tsv, .2d.tsv and .count as one batch."""
+    import shutil
+    work = tempfile.mkdtemp()
+    paths, rows = H.materialise("small", work)
+    outs = []
+    for tag, env in (("one", {}), ("many", {"KGWAS_ROWS_BATCH": "37"})):
+        out = os.path.join(work, tag, "batch_000.tsv")
+        os.makedirs(os.path.dirname(out))
+        r = H.run_cli([paths["samples"], paths["pheno"], rows, paths["ubin"], out, "0", "--log10-thresh-2d", "1",
+                       "--mode", "rows"], dict(env, CORR_THRESHOLD="0"))
+        assert r.returncode == 0, r.stderr[-2000:]
+        outs.append([open(f, "rb").read() for f in (out, O.path_2d(out), out + ".count")])
+    assert outs[0] == outs[1]
+    assert outs[0][0].count(b"\n") > 100
+    shutil.rmtree(work)
+
