@@ -357,6 +357,7 @@ static void run_cols(const Config& cfg) {  // src/kgwas.cpp:168-307
   std::cerr << "[TIME] inputs read " << tall.sec() << " s\n";
 
   g.open(cfg);
+  std::cerr << "[TIME] GPU context ready " << tall.sec() << " s\n";
   kgio::Timer tg;
   double yyM = 0;
   g.check(kg_set_structure(g.ctx, ud.U.data(), n, ud.k, ov.y.data(), &yyM), "set_structure");
@@ -367,6 +368,7 @@ static void run_cols(const Config& cfg) {  // src/kgwas.cpp:168-307
             << ", passed correlation filter: " << res.n_tested << "\n";
   std::cerr << "[INFO] GPU association test (" << tg.sec() << " s, "
             << (cfg.precision == KG_PREC_FP64 ? "fp64" : "split-precision int8 tcgen05") << ")\n";
+  std::cerr << "[TIME] GPU test done " << tall.sec() << " s\n";
 
   kgio::Timer te;
   const bool do_2d = (cfg.log10_thresh_2d > 0.0);
