@@ -337,7 +337,9 @@ void load_matrix_packed(const std::string& bits_dir, const std::vector<int>& idx
       std::cerr << "\r[LOAD] " << d << "/" << n << std::flush;
     }
   }
-  // Transpose 64 sample columns at a time into one word column.
+  // Transpose 64 sample columns at a time into one word column: 8 k-mers x 8
+  // samples per step, each sample's 8 bytes read as one word whose low bits
+  // (the '0'/'1' parity) land in 8 bits of one byte per k-mer.
   const size_t BLK = 8192;
   const size_t nblk = (N + BLK - 1) / BLK;
 #pragma omp parallel
@@ -348,11 +350,28 @@ void load_matrix_packed(const std::string& bits_dir, const std::vector<int>& idx
       const size_t j0 = b * BLK, len = std::min(BLK, N - j0);
       for (uint32_t wc = 0; wc < W; ++wc) {
         std::fill(acc.begin(), acc.begin() + len, 0ull);
-        for (int tt = 0; tt < 64; ++tt) {
-          const int s = (int)wc * 64 + tt;
-          if (s >= n) break;
-          const unsigned char* src = cols[s].p + j0;
-          for (size_t jj = 0; jj < len; ++jj) acc[jj] |= (uint64_t)(src[jj] & 1u) << tt;
+        uint8_t* ab = reinterpret_cast<uint8_t*>(acc.data());  // byte q of a word: samples 8q..8q+7 (little-endian)
+        const size_t len8 = len & ~(size_t)7;
+        for (int q = 0; q < 8; ++q) {
+          const int s0 = (int)wc * 64 + q * 8;
+          if (s0 >= n) break;
+          const int ns = n - s0 < 8 ? n - s0 : 8;
+          const unsigned char* src[8];
+          for (int t = 0; t < 8; ++t) src[t] = cols[s0 + (t < ns ? t : 0)].p + j0;
+          for (size_t jj = 0; jj < len8; jj += 8) {
+            uint64_t w = 0;  // byte b: bit t = sample s0 + t of k-mer j0 + jj + b
+            for (int t = 0; t < ns; ++t) {
+              uint64_t v;
+              std::memcpy(&v, src[t] + jj, 8);
+              w |= (v & 0x0101010101010101ull) << t;
+            }
+            for (int b = 0; b < 8; ++b) ab[(jj + b) * 8 + q] = (uint8_t)(w >> (8 * b));
+          }
+          for (size_t jj = len8; jj < len; ++jj) {
+            uint8_t w = 0;
+            for (int t = 0; t < ns; ++t) w |= (uint8_t)((src[t][jj] & 1u) << t);
+            ab[jj * 8 + q] = w;
+          }
         }
         for (size_t jj = 0; jj < len; ++jj) out[(j0 + jj) * W + wc] = acc[jj];
       }

@@ -429,3 +429,33 @@ def test_rows_reader_short_bitstring(tmp_path):
     assert r.returncode == 1
     assert r.stderr.strip().splitlines()[-1] == "[ERROR] bitstring shorter than the samples list in row: CCC"
 
+
+@pytest.mark.parametrize("N,n_all,threads", [(1003, 77, 1), (20011, 150, 4), (8, 64, 2)])
+def test_column_reader(tmp_path, N, n_all, threads):
+    """The COLS reader (kgio::load_matrix_packed) packs sample idxs[k] of the
+    batch's column files (src/kgwas_utils.hpp:225-282; some columns gzipped)
+    into bit k of each k-mer's row, for k-mer counts and sample counts that
+    are not multiples of 8 or 64."""
+    out_so = os.path.join(HERE, "native", "_build", "libcols_check.so")
+    src = [os.path.join(HERE, "native", "cols_check.cpp"), os.path.join(build.CSRC, "kgwas_io.cpp")]
+    if not os.path.exists(out_so) or any(os.path.getmtime(x) > os.path.getmtime(out_so) for x in src):
+        os.makedirs(os.path.dirname(out_so), exist_ok=True)
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", out_so, *src, "-lz"],
+                       check=True)
+    L = ctypes.CDLL(out_so)
+    vp = ctypes.c_void_p
+    L.cols_read.argtypes = [ctypes.c_char_p, vp, ctypes.c_int, ctypes.c_ulong, ctypes.c_int, vp]
+    rng = np.random.default_rng(N + n_all)
+    x = (rng.random((N, n_all)) < 0.4).astype(np.uint8)
+    packed_all = synth.pack_rows(x)
+    kmers = synth.random_kmers(rng, N, 31)
+    d = str(tmp_path / "batch_000")
+    synth.write_batch(d, packed_all, n_all, kmers, gz_columns=range(0, n_all, 5))
+    idxs = np.sort(rng.choice(n_all, size=n_all - n_all // 7, replace=False)).astype(np.int32)
+    W = synth.words_per_kmer(idxs.size)
+    got = np.zeros((N, W), np.uint64)
+    L.cols_read(os.path.join(d, "bits").encode(), idxs.ctypes.data, idxs.size, N, threads, got.ctypes.data)
+    exp = synth.select_samples(packed_all, n_all, idxs)
+    assert exp.shape == got.shape
+    assert np.array_equal(got, exp)
+
