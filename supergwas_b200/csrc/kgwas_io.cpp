@@ -454,6 +454,20 @@ size_t RowsReader::read(size_t max_rows, const std::vector<int>& idxs, std::vect
   std::vector<size_t> ls, le;  // line spans [ls, le) of this round
   std::vector<size_t> sep;     // separator position (or SIZE_MAX: no row)
   std::vector<size_t> slot;    // output row of each line
+  // the overlap positions as maximal runs of consecutive positions
+  struct IdxRun {
+    int j0;
+    size_t p0;
+    int len;
+  };
+  std::vector<IdxRun> runs;
+  size_t max_pos = 0;
+  for (int j = 0; j < n; ++j) {
+    const size_t pos = (size_t)idxs[j];
+    max_pos = std::max(max_pos, pos);
+    if (!runs.empty() && runs.back().p0 + (size_t)runs.back().len == pos) ++runs.back().len;
+    else runs.push_back({j, pos, 1});
+  }
   while (got < max_rows) {
     ls.clear();
     le.clear();
@@ -528,7 +542,10 @@ size_t RowsReader::read(size_t max_rows, const std::vector<int>& idxs, std::vect
     kmers.resize(k0 + rows);
     packed.resize(p0 + rows * W, 0ull);
     // pass 2: pack the rows; the first row (in file order) whose bitstring is
-    // too short is the error
+    // too short is the error.  Runs of consecutive positions go 8 samples at
+    // a time: the 8 characters as one word, an exact per-byte test for '1'
+    // (xor, then a zero-byte test without borrows between bytes) and one
+    // multiply that gathers the 8 flags into one byte in sample order.
     std::atomic<size_t> bad{SIZE_MAX};
 #pragma omp parallel for num_threads(threads) schedule(static)
     for (int64_t t = 0; t < (int64_t)L; ++t) {
@@ -536,14 +553,24 @@ size_t RowsReader::read(size_t max_rows, const std::vector<int>& idxs, std::vect
       const char* bits = B + sep[t] + 1;
       const size_t nb = le[t] - (sep[t] + 1);
       uint64_t* row = packed.data() + p0 + slot[t] * W;
-      bool ok = true;
-      for (int j = 0; j < n; ++j) {
-        const size_t pos = (size_t)idxs[j];
-        if (pos < nb) {
-          if (bits[pos] == '1') row[j >> 6] |= 1ull << (j & 63);
-        } else if (pos > nb) {
-          ok = false;
-          break;
+      bool ok = max_pos <= nb;  // one past the end reads '\0'
+      for (size_t gi = 0; ok && gi < runs.size(); ++gi) {
+        const IdxRun& g = runs[gi];
+        int k = 0;
+        for (; k + 8 <= g.len && g.p0 + (size_t)k + 8 <= nb; k += 8) {
+          uint64_t v;
+          std::memcpy(&v, bits + g.p0 + k, 8);
+          const uint64_t x = v ^ 0x3131313131313131ull;  // zero bytes where '1'
+          const uint64_t z = ~(((x & 0x7F7F7F7F7F7F7F7Full) + 0x7F7F7F7F7F7F7F7Full) | x | 0x7F7F7F7F7F7F7F7Full);
+          const uint64_t f = (((z >> 7) & 0x0101010101010101ull) * 0x0102040810204080ull) >> 56;
+          const int j = g.j0 + k;
+          row[j >> 6] |= f << (j & 63);
+          if ((j & 63) > 56) row[(j >> 6) + 1] |= f >> (64 - (j & 63));
+        }
+        for (; k < g.len; ++k) {
+          const size_t pos = g.p0 + (size_t)k;
+          const int j = g.j0 + k;
+          if (pos < nb && bits[pos] == '1') row[j >> 6] |= 1ull << (j & 63);
         }
       }
       if (!ok) {

@@ -375,7 +375,7 @@ def test_rows_reader(tmp_path, gz, threads, max_rows):
     for i in range(400):
         k = "".join(rng.choice(list("ACGT"), size=31))
         bits = "".join(rng.choice(["0", "1"], size=n_all))
-        kind = i % 9
+        kind = i % 10
         if kind == 1:
             lines.append("")
         elif kind == 2:
@@ -386,6 +386,8 @@ def test_rows_reader(tmp_path, gz, threads, max_rows):
             lines.append(k + "\t" + bits + "\r")
         elif kind == 5:
             lines.append(k + "\t" + bits[: idxs[-1]])      # one short: reads the terminator
+        elif kind == 6:
+            lines.append(k + "\t" + bits[: idxs[-1]] + "\r")  # the last sample reads the '\\r' (plain)
         else:
             lines.append(k + "\t" + bits)
     text = "\n".join(lines)                                 # no '\\n' after the last line
