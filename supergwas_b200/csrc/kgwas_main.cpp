@@ -204,14 +204,14 @@ static void write_count(const string& out_file, uint64_t n_tested) {  // src/kgw
 // formatting (6 significant digits), k-mer order.  With index1/index2 the rows
 // are also kept for the index writer, with the values as printed (build_index
 // reads them back with strtod, src/build_index.cpp:89-90).
-static void format_hits(const kg_result& r, const vector<string>& kmers, const uint64_t* packed, uint32_t W,
-                        int n, bool do_2d, double p_thresh_2d, string& one, string& two,
-                        vector<kgio::IndexRow>* index1 = nullptr, vector<kgio::IndexRow>* index2 = nullptr) {
+static void format_range(const kg_result& r, uint64_t h0, uint64_t h1, const vector<string>& kmers,
+                         const uint64_t* packed, uint32_t W, int n, bool do_2d, double p_thresh_2d, string& one,
+                         string& two, vector<kgio::IndexRow>* index1, vector<kgio::IndexRow>* index2) {
   std::ostringstream o1, o2, ev, pv;
   o1.setf(std::ios::fmtflags(0), std::ios::floatfield);
   o2.setf(std::ios::fmtflags(0), std::ios::floatfield);
   string bits(n, '0');
-  for (uint64_t h = 0; h < r.n_hits; ++h) {
+  for (uint64_t h = h0; h < h1; ++h) {
     const kg_hit& x = r.hits[h];
     const string& km = kmers[x.kmer];
     const bool is2 = do_2d && x.pval <= p_thresh_2d;
@@ -247,6 +247,37 @@ static void format_hits(const kg_result& r, const vector<string>& kmers, const u
   }
   one = o1.str();
   two = o2.str();
+}
+
+// The hits in `threads` contiguous slices (EMIT_THREADS, src/kgwas.cpp:227-259),
+// each formatted on its own thread and joined in order: the same bytes as one
+// pass.  The index rows are appended to index1 / index2 in row order.
+static void format_hits(const kg_result& r, const vector<string>& kmers, const uint64_t* packed, uint32_t W,
+                        int n, bool do_2d, double p_thresh_2d, string& one, string& two, int threads,
+                        vector<kgio::IndexRow>* index1 = nullptr, vector<kgio::IndexRow>* index2 = nullptr) {
+  const uint64_t H = r.n_hits;
+  const int T = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)std::max(1, threads), H / 256));
+  vector<string> ones(T), twos(T);
+  vector<vector<kgio::IndexRow>> i1(T), i2(T);
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+  for (int t = 0; t < T; ++t)
+    format_range(r, H * t / T, H * (t + 1) / T, kmers, packed, W, n, do_2d, p_thresh_2d, ones[t], twos[t],
+                 index1 ? &i1[t] : nullptr, index2 ? &i2[t] : nullptr);
+  size_t b1 = 0, b2 = 0;
+  for (int t = 0; t < T; ++t) {
+    b1 += ones[t].size();
+    b2 += twos[t].size();
+  }
+  one.clear();
+  two.clear();
+  one.reserve(b1);
+  two.reserve(b2);
+  for (int t = 0; t < T; ++t) {
+    one += ones[t];
+    two += twos[t];
+    if (index1) index1->insert(index1->end(), std::make_move_iterator(i1[t].begin()), std::make_move_iterator(i1[t].end()));
+    if (index2) index2->insert(index2->end(), std::make_move_iterator(i2[t].begin()), std::make_move_iterator(i2[t].end()));
+  }
 }
 
 // Writes one index (build_index on this run's .tsv or .2d.tsv file): k from
@@ -375,7 +406,8 @@ static void run_cols(const Config& cfg) {  // src/kgwas.cpp:168-307
   const double p_thresh_2d = do_2d ? std::pow(10.0, -cfg.log10_thresh_2d) : 0.0;
   string one, two;
   vector<kgio::IndexRow> index1, index2;
-  format_hits(res, kmers, X.p, W, n, do_2d, p_thresh_2d, one, two, cfg.index_out.empty() ? nullptr : &index1,
+  format_hits(res, kmers, X.p, W, n, do_2d, p_thresh_2d, one, two, cfg.EMIT_THREADS,
+              cfg.index_out.empty() ? nullptr : &index1,
               cfg.index_2d_out.empty() ? nullptr : &index2);
   {
     std::ofstream out(cfg.out_file, std::ios::binary);
@@ -480,7 +512,7 @@ static void run_rows(const Config& cfg) {  // src/kgwas.cpp:343-522
     t_gpu += tg.sec();
     passed += res.n_tested;
     string one, two;
-    format_hits(res, cur.kmers, cur.packed.data(), W, n, do_2d, p_thresh_2d, one, two,
+    format_hits(res, cur.kmers, cur.packed.data(), W, n, do_2d, p_thresh_2d, one, two, cfg.EMIT_THREADS,
                 cfg.index_out.empty() ? nullptr : &index1, cfg.index_2d_out.empty() ? nullptr : &index2);
     if (first_kmer.empty() && !cur.kmers.empty()) first_kmer = cur.kmers[0];
     out.write(one.data(), (std::streamsize)one.size());
