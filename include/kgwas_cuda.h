@@ -188,6 +188,21 @@ int kg_launch_multi_device(kg_ctx* ctx, const uint64_t* d_xbits, uint64_t n_kmer
                            void* stream);
 int kg_fetch_multi(kg_ctx* ctx, kg_multi_result* res);
 
+/* Tile shape of the many-phenotype launches, as kg_set_phenotypes and the
+ * autotuner chose it (this build's own batching; the reference runs one
+ * process per phenotype and batch, HPC/kgwas/kgwas_cols.sh:22-65). */
+typedef struct kg_tile_shape {
+    int kernel;   /* 1: each group's limb image resident in shared memory;
+                     2: images streamed from L2                              */
+    int np;       /* limb columns per phenotype slot                         */
+    int ppg;      /* phenotypes per MMA group (MMA N = np * ppg)             */
+    int groups;   /* MMA groups                                              */
+    int kpad;     /* samples per image (padded)                              */
+    int bt;       /* kernel 1: tile-iterations per L2 block of the last launch */
+    int xs, nb;   /* kernel 2: resident row tiles, image ring stages         */
+} kg_tile_shape;
+int kg_multi_shape(const kg_ctx* ctx, kg_tile_shape* out);
+
 /* Same from host rows (chunked host-to-device copies overlapped with the kernels). */
 int kg_run_multi_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t n_kmers, uint32_t words_per_kmer,
                       const uint64_t* shard_start, int n_shards, kg_multi_result* res);
@@ -243,11 +258,37 @@ const char* kg_last_kernel(const kg_ctx* ctx);
  * for pinned rows too. */
 uint64_t kg_last_unique_rows(const kg_ctx* ctx);
 
+/* Bounded device-side waits.  Every wait between the roles of the
+ * association kernels' pipelines (row loads, tensor-memory slots,
+ * accumulators) gives up after wait_ns nanoseconds: the kernel then stops,
+ * waits for its own copies and MMAs in flight, frees its tensor memory and
+ * returns, and the call reports KG_ERR_TIMEOUT while the context stays
+ * usable.  0 restores the default of 2 s.  The reference has no device waits;
+ * its failures end the process (die(), src/kgwas_utils.hpp:34-37). */
+int kg_set_wait_limit(kg_ctx* ctx, uint64_t wait_ns);
+
+/* Failure test hook of the bounded waits, off by default: for the next
+ * launch of the single-phenotype tensor-memory kernel only, the row producer
+ * of every CTA issues its first stop_after_loads row loads and then no more,
+ * so that the waits of the roles it feeds run out (KG_ERR_TIMEOUT) instead of
+ * completing.  No counterpart in the reference. */
+int kg_inject_stall(kg_ctx* ctx, uint64_t stop_after_loads);
+
 const char* kg_last_error(const kg_ctx* ctx);
 void kg_destroy(kg_ctx* ctx);
 
 /* Library version string. */
 const char* kg_version(void);
+
+/* Measured peaks that throughput figures are reported against; no
+ * counterpart in the reference.  kg_probe_fp64_tflops: FP64 FMA rate of the
+ * CUDA cores (independent FMA chains on every SM), in TFLOP/s -- the bound of
+ * the KG_PREC_FP64 form.  kg_probe_h2d_gbs: pinned host-to-device copy rate,
+ * `reps` copies of `bytes` with one cudaMemcpyAsync each, in GB/s -- the
+ * bound of kg_run_host / kg_run_multi_host on rows from host memory.  Both
+ * allocate their own buffers and synchronise. */
+int kg_probe_fp64_tflops(int device, double* tflops);
+int kg_probe_h2d_gbs(int device, uint64_t bytes, int reps, double* gbs);
 
 /* Allocation-free run, for callers that may not allocate device memory (a
  * host framework that owns every device byte through its own pool, a plugin
@@ -255,24 +296,36 @@ const char* kg_version(void);
  * in the reference.
  *
  * Runs the split-precision test of kg_set_structure + kg_launch_device in one
- * call, without a context: d_xbits (device, packed rows as above), U/y (host,
- * as in kg_set_structure), and d_hits (device, hit_capacity records, filled
- * in arbitrary order).  counts_out (host) receives {n_tested, n_hits}.  The
- * call is synchronous on `stream` (a cudaStream_t, NULL = default stream).
+ * call, without a context, with the same accuracy: k-mers whose split-form
+ * chi-square reaches 12 are recomputed in FP64 before their rows are
+ * emitted.  d_xbits (device, packed rows as above), U/y (host, as in
+ * kg_set_structure), and d_hits (device, hit_capacity records, filled in
+ * arbitrary order).  counts_out (host) receives {n_tested, n_hits}.  The call
+ * blocks: it synchronises `stream` (a cudaStream_t, NULL = default stream)
+ * before it returns.
  *
- * It calls no device allocator.  Its device scratch (the int8 limb image of
- * the structure and the counters) is one static array of
- * KG_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds until
- * the process exits; structures whose image exceeds KG_NOALLOC_MAX_B_BYTES
- * (overlap samples rounded up to 256, times the limb columns rounded up to 16)
- * are rejected with KG_ERR_UNSUPPORTED.  The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress) and should come before
- * any stream capture on that device.  Calls share the array: calls that
- * overlap on the GPU race and must be serialised by the caller.  More hits
- * than hit_capacity return KG_ERR_INVALID with counts_out still filled.
- * err (optional, err_len bytes) receives a message on failure. */
+ * It calls no device allocator.  Its device scratch (the counters, the int8
+ * limb image of the structure, the FP64 columns of the refinement and the
+ * list of k-mers to refine) is one static array of KG_NOALLOC_SCRATCH_BYTES
+ * that every GPU loading this library holds until the process exits.
+ * Structures whose limb image exceeds KG_NOALLOC_MAX_B_BYTES (overlap samples
+ * rounded up to 256, times the limb columns rounded up to 16) or whose FP64
+ * columns exceed KG_NOALLOC_MAX_V_BYTES (overlap samples rounded up to 128,
+ * times k + 2 columns rounded up to 8..68, times 8 bytes) are rejected with
+ * KG_ERR_UNSUPPORTED.  At most KG_NOALLOC_MAX_REFINE k-mers are refined per
+ * pass; a batch with more is run again in smaller pieces.  The first call on
+ * a device (and the first after that device's context was destroyed and
+ * created anew) looks up the array's device address with
+ * cudaGetSymbolAddress; make it before any stream capture on that device.
+ * Calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  More hits than hit_capacity return
+ * KG_ERR_INVALID with counts_out still filled.  err (optional, err_len bytes)
+ * receives a message on failure. */
 #define KG_NOALLOC_MAX_B_BYTES (256u * 1024u)
-#define KG_NOALLOC_SCRATCH_BYTES (KG_NOALLOC_MAX_B_BYTES + 256u)
+#define KG_NOALLOC_MAX_V_BYTES (1024u * 1024u)
+#define KG_NOALLOC_MAX_REFINE 32768u
+#define KG_NOALLOC_SCRATCH_BYTES \
+    (256u + KG_NOALLOC_MAX_B_BYTES + KG_NOALLOC_MAX_V_BYTES + 8u * KG_NOALLOC_MAX_REFINE)
 int kg_run_device_noalloc(const uint64_t* d_xbits, uint64_t n_kmers, uint32_t words_per_kmer,
                           const double* U_colmajor, int n, int k, const double* y,
                           double corr_threshold, double log10_thresh,

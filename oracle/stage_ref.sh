@@ -9,7 +9,7 @@
 # the Python environment's opencv wheel (symlinked as libopenblas.so.0).
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:?usage: stage_ref.sh REFERENCE_DIR (the reference checkout holding bin/kgwas)}"
 OUT="$HERE/_ref"
 if [[ ! -x "$REF/bin/kgwas" ]]; then
   echo "reference binary not found at $REF/bin/kgwas" >&2

@@ -74,6 +74,11 @@ PAIR_DTYPE = np.dtype([("a", np.uint64), ("b", np.uint64), ("effect", np.float64
                        ("chisq", np.float64)])
 
 
+class _TileShape(ctypes.Structure):
+    _fields_ = [("kernel", ctypes.c_int), ("np", ctypes.c_int), ("ppg", ctypes.c_int), ("groups", ctypes.c_int),
+                ("kpad", ctypes.c_int), ("bt", ctypes.c_int), ("xs", ctypes.c_int), ("nb", ctypes.c_int)]
+
+
 class _PairResult(ctypes.Structure):
     _fields_ = [("n_kmers", ctypes.c_uint64), ("n_evaluated", ctypes.c_uint64), ("n_pairs", ctypes.c_uint64),
                 ("pairs", ctypes.c_void_p)]
@@ -118,6 +123,11 @@ def lib():
     L.kg_last_error.restype = ctypes.c_char_p
     L.kg_destroy.argtypes = [vp]
     L.kg_destroy.restype = None
+    L.kg_probe_fp64_tflops.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.kg_probe_h2d_gbs.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.kg_multi_shape.argtypes = [vp, ctypes.POINTER(_TileShape)]
+    L.kg_set_wait_limit.argtypes = [vp, ctypes.c_uint64]
+    L.kg_inject_stall.argtypes = [vp, ctypes.c_uint64]
     L.kg_version.restype = ctypes.c_char_p
     L.kg_host_alloc.argtypes = [ctypes.c_size_t]
     L.kg_host_alloc.restype = vp
@@ -329,11 +339,30 @@ class Kgwas:
                                               sp, ns, ctypes.byref(r)), "kg_run_multi_host")
         return self._multi_result(r)
 
+    def multi_shape(self) -> dict:
+        """Tile shape of the many-phenotype launches (kg_multi_shape)."""
+        t = _TileShape()
+        self._check(self._L.kg_multi_shape(self._h, ctypes.byref(t)), "kg_multi_shape")
+        d = {f: int(getattr(t, f)) for f, _ in _TileShape._fields_}
+        d["kernel"] = {1: "image resident (mpb)", 2: "image streamed (mp)"}.get(d["kernel"], d["kernel"])
+        d["NP"] = d.pop("np")
+        d["PPG"] = d.pop("ppg")
+        d["N"] = d["NP"] * d["PPG"]
+        return d
+
     def last_launch_count(self) -> int:
         return int(self._L.kg_last_launch_count(self._h))
 
     def last_kernel(self) -> str:
         return self._L.kg_last_kernel(self._h).decode()
+
+    def set_wait_limit(self, wait_ns: int):
+        """Limit of every pipeline wait on the device, in ns (0: the default 2 s)."""
+        self._check(self._L.kg_set_wait_limit(self._h, int(wait_ns)), "kg_set_wait_limit")
+
+    def inject_stall(self, stop_after_loads: int):
+        """Failure-test hook: the next launch's row producer stops after this many loads per CTA."""
+        self._check(self._L.kg_inject_stall(self._h, int(stop_after_loads)), "kg_inject_stall")
 
     def last_unique_rows(self) -> int:
         """Rows the last run_host tested when it used runs of equal adjacent rows (0: every row)."""
@@ -357,6 +386,24 @@ def run_device_noalloc(d_x: int, m: int, wpk: int, U, y, corr_threshold: float, 
                                      corr_threshold, log10_thresh, d_hits, hit_capacity, counts, stream,
                                      msg, len(msg))
     return rc, int(counts[0]), int(counts[1]), msg.value.decode()
+
+
+def probe_fp64_tflops(device: int = 0) -> float:
+    """Measured FP64 FMA rate of the CUDA cores (TFLOP/s)."""
+    v = ctypes.c_double()
+    rc = lib().kg_probe_fp64_tflops(device, ctypes.byref(v))
+    if rc != KG_OK:
+        raise KgError(rc, "kg_probe_fp64_tflops")
+    return v.value
+
+
+def probe_h2d_gbs(device: int = 0, nbytes: int = 1 << 30, reps: int = 8) -> float:
+    """Measured pinned host-to-device copy rate (GB/s)."""
+    v = ctypes.c_double()
+    rc = lib().kg_probe_h2d_gbs(device, nbytes, reps, ctypes.byref(v))
+    if rc != KG_OK:
+        raise KgError(rc, "kg_probe_h2d_gbs")
+    return v.value
 
 
 def version() -> str:

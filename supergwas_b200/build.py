@@ -24,11 +24,10 @@ LIB = os.path.join(LIB_DIR, "libkgwas_cuda.so")
 CLI = os.path.join(BIN_DIR, "kgwas")
 CLI2 = os.path.join(BIN_DIR, "kgwas_2d")
 MERGE = os.path.join(BIN_DIR, "kgwas_index_merge")
-MMA_RATE = os.path.join(BIN_DIR, "mma_rate")
 OBJ_DIR = os.path.join(PKG, "_build")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-LIB_SOURCES = ["kernels.cu", "kernel_ts.cu", "kernel_mp.cu", "kernel_mpb.cu", "kernel_pairs.cu", "capi_pairs.cpp", "noalloc.cu", "capi.cpp", "capi_multi.cpp", "prep.cpp"]
+LIB_SOURCES = ["kernels.cu", "kernel_ts.cu", "kernel_mp.cu", "kernel_mpb.cu", "kernel_pairs.cu", "capi_pairs.cpp", "noalloc.cu", "probes.cu", "capi.cpp", "capi_multi.cpp", "prep.cpp"]
 CLI_SOURCES = ["kgwas_main.cpp", "kgwas_io.cpp"]
 CLI2_SOURCES = ["kgwas2d_main.cpp", "kgwas_io.cpp"]
 MERGE_SOURCES = ["index_merge_main.cpp", "kgwas_io.cpp"]
@@ -101,22 +100,11 @@ def build_cli(force=False, verbose=False, target=None, sources=None) -> str:
     return target
 
 
-def build_mma_rate(force=False, verbose=False) -> str:
-    """The tensor-core rate measurement program (bin/mma_rate)."""
-    src = os.path.join(CSRC, "mma_rate.cu")
-    if not force and _newer(MMA_RATE, [src, os.path.join(CSRC, "device.cuh")]):
-        return MMA_RATE
-    os.makedirs(BIN_DIR, exist_ok=True)
-    run([nvcc(), *ARCH, "-O3", "-std=c++17", "-o", MMA_RATE, src], verbose)
-    return MMA_RATE
-
-
 def build_all(force=False, verbose=False):
     build_lib(force, verbose)
     build_cli(force, verbose)
     build_cli(force, verbose, CLI2, CLI2_SOURCES)
     build_cli(force, verbose, MERGE, MERGE_SOURCES)
-    build_mma_rate(force, verbose)
     return LIB, CLI
 
 

@@ -117,6 +117,18 @@ int kg_last_launch_count(const kg_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 const char* kg_last_kernel(const kg_ctx* ctx) { return ctx ? ctx->last_kernel : ""; }
 
+int kg_set_wait_limit(kg_ctx* ctx, uint64_t wait_ns) {
+  if (!ctx) return KG_ERR_INVALID;
+  ctx->wait_ns = wait_ns;
+  return KG_OK;
+}
+
+int kg_inject_stall(kg_ctx* ctx, uint64_t stop_after_loads) {
+  if (!ctx) return KG_ERR_INVALID;
+  ctx->stall_once = stop_after_loads;
+  return KG_OK;
+}
+
 int kg_set_structure_ex(kg_ctx* ctx, const double* U, int n, int k, const double* y, const int32_t* sample_pos,
                         int n_row_samples, double* yyM_out) {
   if (!ctx) return KG_ERR_INVALID;
@@ -460,6 +472,9 @@ int launch_one(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, uint64
   O.cand = ctx->dCand;
   O.cand_cap = ctx->cand_cap;
   O.weight = ctx->cur_weight;
+  O.wait_ns = ctx->wait_ns;
+  O.stall_loads = ctx->stall_once;
+  ctx->stall_once = 0;
   if (stats) {
     O.tested = ctx->dTested;
     O.chisq = ctx->dStat[0];

@@ -134,6 +134,7 @@ int enqueue_multi(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, uns
     unsigned long long bt = (48ull << 20) / std::max<unsigned long long>(1, grid * tile_bytes);
     if (const char* v = std::getenv("KG_MP_BT")) bt = (unsigned long long)std::max(1, std::atoi(v));
     bt = std::max<unsigned long long>(1, std::min<unsigned long long>(bt, 1024));
+    M.bt = (int)bt;
     kg::LaunchMpb L{dx, m, (int)wpk, M.kpad, M.NP, M.PPG, M.G, (int)bt, M.dB, M.dPh, &O, ctx->num_sms};
     e = kg::launch_mpb(L, st);
   } else {
@@ -360,6 +361,21 @@ int kg_set_phenotypes(kg_ctx* ctx, const kg_pheno* ph, int np, int n_row) {
   kg::LaunchTable LT{M.dV, vrows, cm, (unsigned long long)M.vstride, np, M.dT};
   KG_CUDA(kg::launch_refine_table(LT, ctx->stream), "refinement tables");
   KG_CUDA(cudaStreamSynchronize(ctx->stream), "refinement tables");
+  return KG_OK;
+}
+
+int kg_multi_shape(const kg_ctx* ctx, kg_tile_shape* out) {
+  if (!ctx || !out) return KG_ERR_INVALID;
+  const Multi& M = ctx->mp;
+  if (M.np <= 0) return KG_ERR_STATE;
+  out->kernel = M.stationary ? 1 : 2;
+  out->np = M.NP;
+  out->ppg = M.PPG;
+  out->groups = M.G;
+  out->kpad = M.kpad;
+  out->bt = M.bt;
+  out->xs = M.xs;
+  out->nb = M.nb;
   return KG_OK;
 }
 

@@ -85,6 +85,7 @@ struct Multi {
   unsigned long long counters[4] = {0, 0, 0, 0};
   // launch shape chosen by the autotuner: x tiles resident, B ring stages
   int xs = 1, nb = 4;
+  int bt = 0;  // B-stationary kernel: tile-iterations per L2 block of the last launch
   bool tuned = false;
   int tuned_nbox = -1;
   // pending device launch and its captured graph
@@ -142,6 +143,10 @@ struct kg_ctx {
   cudaStream_t pend_stream = nullptr;
   int launches = 0;
   const char* last_kernel = "";
+  // bounded device waits: pipeline wait limit (0: the default) and the
+  // one-launch stall of the row producer that the failure tests use
+  unsigned long long wait_ns = 0;
+  unsigned long long stall_once = 0;
   // host-run buffers
   uint64_t* dChunk[kgctx::NBUF] = {};
   void* hStage[kgctx::NBUF] = {};

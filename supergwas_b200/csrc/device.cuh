@@ -224,22 +224,32 @@ __device__ __forceinline__ void unpack_stage(const uint32_t (&w)[4], uint32_t (&
 
 // Bounded wait that also gives up when another role has aborted.  The first
 // test is inline (the common case: the phase is already complete); the
-// abort flag and the clock are read only every 16 failed tests.
+// abort flag and the clock are read only every 16 failed tests.  limit_ns:
+// how long to wait before giving up (a launch parameter, see wait_limit).
 __device__ __forceinline__ bool wait_or_abort(uint32_t bar, uint32_t parity, volatile int* abort,
-                                        unsigned long long* counters, unsigned code) {
+                                        unsigned long long* counters, unsigned code,
+                                        unsigned long long limit_ns = WAIT_LIMIT_NS) {
   if (mbar_try(bar, parity)) return true;
   const unsigned long long t0 = gtimer_ns();
   for (uint32_t it = 1;; ++it) {
     if (mbar_try_sleep(bar, parity)) return true;
     if ((it & 15u) == 0) {
       if (*abort) return false;
-      if (gtimer_ns() - t0 > WAIT_LIMIT_NS) {
+      if (gtimer_ns() - t0 > limit_ns) {
         atomicOr(counters + 2, (unsigned long long)code);
         *abort = 1;
         return false;
       }
     }
   }
+}
+
+// The pipeline wait limit of a launch: the caller's value, or WAIT_LIMIT_NS
+// when it left it at 0.  Only the waits between the roles of a pipeline use
+// it; the final waits for a CTA's own copies and MMAs always allow
+// WAIT_LIMIT_NS, so that nothing is still landing when a CTA exits.
+__device__ __forceinline__ unsigned long long wait_limit(unsigned long long ns) {
+  return ns ? ns : WAIT_LIMIT_NS;
 }
 
 // Ring position: slot index and phase parity, advanced without division.

@@ -135,6 +135,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
   const unsigned long long ntiles = (m + TS_TM - 1) / TS_TM;
+  const unsigned long long lim = wait_limit(O.wait_ns);
 
   if (warp == TS_WARP_PROD) {
     // ------------------------------------------------------------ producer
@@ -150,9 +151,14 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
       bool issued[TS_XST_MAX];
       for (int s = 0; s < TS_XST_MAX; ++s) issued[s] = false, last_phase[s] = 0;
       bool ok = true;
+      unsigned long long loads = 0;
       for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         for (int bx = 0; bx < nbox; ++bx, xr.next()) {
-          if (xr.used && !wait_or_abort(x_empty + 8 * xr.slot, xr.phase ^ 1u, s_abort, O.counters, ERR_TIMEOUT_FULL)) {
+          if (xr.used && !wait_or_abort(x_empty + 8 * xr.slot, xr.phase ^ 1u, s_abort, O.counters, ERR_TIMEOUT_FULL, lim)) {
+            ok = false;
+            break;
+          }
+          if (O.stall_loads && loads++ == O.stall_loads) {  // test hook: stop feeding the pipeline
             ok = false;
             break;
           }
@@ -172,21 +178,21 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
     // The whole warp runs the loop (warp-uniform control flow and operands);
     // one elected lane issues the MMAs and the commits that track them.
     const bool leader = elect_one();
-    bool ok = __all_sync(0xffffffffu, wait_or_abort(b_full, 0, s_abort, O.counters, ERR_TIMEOUT_FULL));
+    bool ok = __all_sync(0xffffffffu, wait_or_abort(b_full, 0, s_abort, O.counters, ERR_TIMEOUT_FULL, lim));
     const uint64_t bdesc0 = sdesc_noswz(sb, N * 16, 128);
     Ring<NSLOT> ar;
     uint32_t i = 0;
     for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++i) {
       const uint32_t b = i & 1u;
       if (i >= 2 && !__all_sync(0xffffffffu, wait_or_abort(acc_empty + 8 * b, ((i >> 1) - 1) & 1u, s_abort, O.counters,
-                                                     ERR_TIMEOUT_MMA))) {
+                                                     ERR_TIMEOUT_MMA, lim))) {
         ok = false;
         break;
       }
       const uint32_t d_t = tmem + b * N;
       uint64_t bd = bdesc0;
       for (int sp = 0; sp < nsp; ++sp, ar.next()) {
-        if (!__all_sync(0xffffffffu, wait_or_abort(a_full + 8 * ar.slot, ar.phase, s_abort, O.counters, ERR_TIMEOUT_MMA))) {
+        if (!__all_sync(0xffffffffu, wait_or_abort(a_full + 8 * ar.slot, ar.phase, s_abort, O.counters, ERR_TIMEOUT_MMA, lim))) {
           ok = false;
           break;
         }
@@ -240,7 +246,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
         // every unpack warp waits for every box, also one holding none of its
         // super-stages, so that its release below belongs to this fill
         if (!__all_sync(0xffffffffu, wait_or_abort(x_full + 8 * xr.slot, xr.phase, s_abort, O.counters,
-                                            ERR_TIMEOUT_FULL))) {
+                                            ERR_TIMEOUT_FULL, lim))) {
           ok = false;
           break;
         }
@@ -255,7 +261,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
             continue;
           }
           if (ar.used && !__all_sync(0xffffffffu, wait_or_abort(a_empty + 8 * ar.slot, ar.phase ^ 1u, s_abort,
-                                                          O.counters, ERR_TIMEOUT_MMA))) {
+                                                          O.counters, ERR_TIMEOUT_MMA, lim))) {
             ok = false;
             break;
           }
@@ -318,7 +324,7 @@ __global__ void __launch_bounds__(ts_threads(N), 1)
     uint32_t tested_local = 0;  // k-mers this thread tested (lean path)
     for (unsigned long long tile = blockIdx.x + (unsigned long long)e * gridDim.x; tile < ntiles;
          tile += 2ull * gridDim.x, ++jt) {
-      if (!__all_sync(0xffffffffu, wait_or_abort(acc_full + 8 * e, jt & 1u, s_abort, O.counters, ERR_TIMEOUT_MMA))) break;
+      if (!__all_sync(0xffffffffu, wait_or_abort(acc_full + 8 * e, jt & 1u, s_abort, O.counters, ERR_TIMEOUT_MMA, lim))) break;
       tc_fence_after();
       // all N columns in flight at once, then one wait
       uint32_t d[N];

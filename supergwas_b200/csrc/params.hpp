@@ -55,6 +55,12 @@ struct DevOut {
   // optional: a tested k-mer counts weight[kmer_offset + local] times in
   // counters[0] (a row that stands for a run of equal rows)
   const uint32_t* weight;
+  // pipeline wait limit in ns (0: WAIT_LIMIT_NS)
+  unsigned long long wait_ns;
+  // test hook of the bounded waits: when non-zero, the row producer of each
+  // CTA issues this many row loads and then stops, so that the consumers'
+  // waits run out (0: off)
+  unsigned long long stall_loads;
 };
 
 enum : unsigned { ERR_TIMEOUT_FULL = 1u, ERR_TIMEOUT_MMA = 2u, ERR_HIT_OVERFLOW = 4u, ERR_CAND_OVERFLOW = 8u };
@@ -87,6 +93,10 @@ struct DevOutMP {
   // optional: a tested (k-mer, phenotype) counts weight[global k-mer] times
   // (a row that stands for a run of equal rows)
   const uint32_t* weight;
+  // pipeline wait limit in ns (0: WAIT_LIMIT_NS)
+  unsigned long long wait_ns;
+  // test hook of the bounded waits, as DevOut::stall_loads (0: off)
+  unsigned long long stall_loads;
 };
 
 // Outputs of the 2-D pair test (kernel_pairs.cu).

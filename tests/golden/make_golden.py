@@ -623,7 +623,7 @@ def make_pairs():
 
 if __name__ == "__main__":
     if not O.ref_available():
-        sys.exit("stage the reference first: bash oracle/stage_ref.sh")
+        sys.exit("stage the reference first: bash oracle/stage_ref.sh REFERENCE_DIR")
     names = sys.argv[1:] or [*FIXTURES, "cfg1", "faults", "pairs", "pair_faults", "index"]
     for nm in names:
         if nm == "cfg1":

@@ -65,6 +65,33 @@ def test_noalloc_matches_existing_entry_point_twice():
     _same(hits, ref2.hits)
 
 
+def test_noalloc_strong_hits_match_fp64_oracle():
+    """Rows far above the default cut (chi-square in the hundreds, p <= 1e-6)
+    come out of the FP64 refinement: their -log10 p agrees with the FP64
+    oracle to 1e-8, where the split form alone is off by about 1e-5 at these
+    chi-square values.  Every tested k-mer agrees to the parity bar (1e-6)."""
+    from oracle import oracle as O
+    ds = synth.simulate(n=1000, m=20000, S=8, r=16, n_causal=20, missing=0.05, seed=34)
+    X = ds.packed_overlap()
+    x = synth.unpack_rows(X[:16], ds.n).astype(np.float64)
+    y = ds.y + 3.0 * x[3] - 2.5 * x[7] + 2.0 * x[11]
+    o = O.cols_stats(X, ds.n, ds.U, y, 0.0)
+    for call in range(2):  # the second call reuses the scratch the first left behind
+        rc, nt, hits, msg = _device_call(X, ds.U, y, 0.0, 6.0, 4096)
+        assert rc == 0, msg
+        assert nt == o["n_tested"]
+        exp = np.nonzero(o["tested"] & (o["pval"] <= 1e-6))[0]
+        band = np.abs(o["mlog10p"] - 6.0) <= 1e-6
+        got = hits["kmer"].astype(np.int64)
+        assert set(got.tolist()) ^ set(exp.tolist()) <= set(np.nonzero(band)[0].tolist())
+        T0 = o["chisq"][got]
+        assert T0.min() >= 23.0 and T0.max() > 300.0
+        ml = np.abs(O.mlog10p(hits["chisq"]) - o["mlog10p"][got])
+        assert ml.max() <= 1e-8, ml.max()
+        assert np.allclose(hits["chisq"], T0, rtol=1e-10, atol=0.0)
+        assert np.allclose(hits["effect"], o["effect"][got], rtol=1e-9, atol=0.0)
+
+
 def test_noalloc_rejects_oversized_structure():
     # 5000 overlap samples and U with 34 columns: the limb image (5120 x 112) exceeds 256 KiB
     rng = np.random.default_rng(1)
