@@ -193,7 +193,9 @@ int kg_fetch_multi(kg_ctx* ctx, kg_multi_result* res);
  * process per phenotype and batch, HPC/kgwas/kgwas_cols.sh:22-65). */
 typedef struct kg_tile_shape {
     int kernel;   /* 1: each group's limb image resident in shared memory;
-                     2: images streamed from L2                              */
+                     2: images streamed from L2;
+                     3: pairs of SMs (cta_group::2), two phenotypes per M = 256
+                        MMA, one phenotype's image resident in each SM       */
     int np;       /* limb columns per phenotype slot                         */
     int ppg;      /* phenotypes per MMA group (MMA N = np * ppg)             */
     int groups;   /* MMA groups                                              */

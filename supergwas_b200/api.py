@@ -344,7 +344,8 @@ class Kgwas:
         t = _TileShape()
         self._check(self._L.kg_multi_shape(self._h, ctypes.byref(t)), "kg_multi_shape")
         d = {f: int(getattr(t, f)) for f, _ in _TileShape._fields_}
-        d["kernel"] = {1: "image resident (mpb)", 2: "image streamed (mp)"}.get(d["kernel"], d["kernel"])
+        d["kernel"] = {1: "image resident (mpb)", 2: "image streamed (mp)",
+                       3: "SM pair, cta_group::2 (mpb2)"}.get(d["kernel"], d["kernel"])
         d["NP"] = d.pop("np")
         d["PPG"] = d.pop("ppg")
         d["N"] = d["NP"] * d["PPG"]

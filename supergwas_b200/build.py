@@ -27,7 +27,7 @@ MERGE = os.path.join(BIN_DIR, "kgwas_index_merge")
 OBJ_DIR = os.path.join(PKG, "_build")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-LIB_SOURCES = ["kernels.cu", "kernel_ts.cu", "kernel_mp.cu", "kernel_mpb.cu", "kernel_pairs.cu", "capi_pairs.cpp", "noalloc.cu", "probes.cu", "capi.cpp", "capi_multi.cpp", "prep.cpp"]
+LIB_SOURCES = ["kernels.cu", "kernel_ts.cu", "kernel_mp.cu", "kernel_mpb.cu", "kernel_mpb2.cu", "kernel_pairs.cu", "capi_pairs.cpp", "noalloc.cu", "probes.cu", "capi.cpp", "capi_multi.cpp", "prep.cpp"]
 CLI_SOURCES = ["kgwas_main.cpp", "kgwas_io.cpp"]
 CLI2_SOURCES = ["kgwas2d_main.cpp", "kgwas_io.cpp"]
 MERGE_SOURCES = ["index_merge_main.cpp", "kgwas_io.cpp"]

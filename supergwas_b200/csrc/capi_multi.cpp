@@ -125,18 +125,19 @@ int enqueue_multi(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, uns
   kg::DevOutMP O = dev_out(ctx, offset);
   KG_CUDA(cudaMemsetAsync(M.dCounters + 3, 0, sizeof(unsigned long long), st), "memset");
   cudaError_t e;
-  if (M.stationary) {
+  if (M.kern >= 1) {
     // tile-iterations per block: the block's packed rows (every CTA's) stay in L2
-    // across the G passes
+    // across the G passes; the autotuner scales the 48 MB rule by bt_scale / 2
     const unsigned long long tiles = (m + 127) / 128;
     const unsigned long long grid = std::min<unsigned long long>(tiles, (unsigned long long)ctx->num_sms);
     const unsigned long long tile_bytes = 128ull * wpk * 8;
-    unsigned long long bt = (48ull << 20) / std::max<unsigned long long>(1, grid * tile_bytes);
+    unsigned long long bt = (48ull << 20) * (unsigned long long)M.bt_scale / 2 /
+                            std::max<unsigned long long>(1, grid * tile_bytes);
     if (const char* v = std::getenv("KG_MP_BT")) bt = (unsigned long long)std::max(1, std::atoi(v));
     bt = std::max<unsigned long long>(1, std::min<unsigned long long>(bt, 1024));
     M.bt = (int)bt;
     kg::LaunchMpb L{dx, m, (int)wpk, M.kpad, M.NP, M.PPG, M.G, (int)bt, M.dB, M.dPh, &O, ctx->num_sms};
-    e = kg::launch_mpb(L, st);
+    e = M.kern == 2 ? kg::launch_mpb2(L, st) : kg::launch_mpb(L, st);
   } else {
     kg::LaunchMp L{dx, m, (int)wpk, M.kpad, M.NP, M.PPG, M.G, M.xs, M.nb, 0, 0, M.dB, M.dPh, &O, ctx->num_sms};
     e = kg::launch_mp(L, st);
@@ -156,37 +157,59 @@ int reset_outputs(kg_ctx* ctx, cudaStream_t st) {
   return KG_OK;
 }
 
-// Autotuner: time each (resident x tiles, B ring stages) shape on a prefix of
-// the rows and keep the fastest for this row width.
+// Autotuner.  Times candidate launch shapes on a prefix of the rows (up to
+// 148 x 256 x 48 k-mers, every phenotype) and keeps the fastest for this row
+// width:
+//   image resident in shared memory: the one-SM kernel (mpb, PPG phenotypes
+//   per MMA) and, where one phenotype fills an MMA group, the SM-pair kernel
+//   (mpb2, two phenotypes per M = 256 MMA), each with L2 blocks of 0.5x, 1x
+//   and 2x the 48 MB rule;
+//   image streamed from L2 (mp): resident x tiles x B ring stages.
+// KG_MP_KERNEL=mp|mpb|mpb2 restricts the search to one kernel.
 int autotune(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, cudaStream_t st) {
   Multi& M = ctx->mp;
   const int nbox = ((int)wpk * 8 + 127) / 128;
   if (M.tuned && M.tuned_nbox == nbox) return KG_OK;
-  if (M.stationary) {  // the B-stationary kernel has no ring shape to choose
+  struct Cand {
+    int kern, xs, nb, bt_scale;
+  };
+  std::vector<Cand> cands;
+  const char* only = std::getenv("KG_MP_KERNEL");
+  auto allowed = [&](const char* k) { return !only || std::string(only) == k; };
+  if (M.stationary && !(only && std::string(only) == "mp")) {
+    for (int s : {2, 1, 4}) {
+      if (allowed("mpb")) cands.push_back({1, 1, 4, s});
+      if (M.pair_ok && allowed("mpb2")) cands.push_back({2, 1, 4, s});
+    }
+    if (cands.empty()) cands.push_back({1, 1, 4, 2});  // the requested kernel does not fit these phenotypes
+  }
+  if (cands.empty()) {
+    if (const char* v = std::getenv("KG_MP_SHAPE")) {  // "xs,nb": fixed shape, no tuning
+      int xs = 1, nb = 4;
+      if (std::sscanf(v, "%d,%d", &xs, &nb) == 2) cands.push_back({0, std::max(1, std::min(2, xs)), std::max(2, std::min(8, nb)), 2});
+    }
+    if (cands.empty())
+      for (const Cand& c : {Cand{0, 1, 4, 2}, Cand{0, 1, 8, 2}, Cand{0, 2, 4, 2}, Cand{0, 2, 8, 2}}) cands.push_back(c);
+  }
+  if (cands.size() == 1) {
+    M.kern = cands[0].kern;
+    M.bt_scale = cands[0].bt_scale;
+    pick_shape(M, nbox, cands[0].xs, cands[0].nb);
     M.tuned = true;
     M.tuned_nbox = nbox;
     return KG_OK;
   }
-  if (const char* v = std::getenv("KG_MP_SHAPE")) {  // "xs,nb": fixed shape, no tuning
-    int xs = 1, nb = 4;
-    if (std::sscanf(v, "%d,%d", &xs, &nb) == 2) {
-      pick_shape(M, nbox, std::max(1, std::min(2, xs)), std::max(2, std::min(8, nb)));
-      M.tuned = true;
-      M.tuned_nbox = nbox;
-      return KG_OK;
-    }
-  }
-  const uint64_t sample = std::min<uint64_t>(m, (uint64_t)ctx->num_sms * 128 * 16);
-  struct Cand { int xs, nb; };
-  const Cand cands[] = {{1, 4}, {1, 8}, {2, 4}, {2, 8}};
+  const uint64_t sample = std::min<uint64_t>(m, (uint64_t)ctx->num_sms * 256 * 48);
   cudaEvent_t a, b;
   KG_CUDA(cudaEventCreate(&a), "event");
   KG_CUDA(cudaEventCreate(&b), "event");
   float best = 1e30f;
-  int bxs = 1, bnb = 4;
+  Cand win = cands[0];
   for (const Cand& c : cands) {
+    M.kern = c.kern;
+    M.bt_scale = c.bt_scale;
     pick_shape(M, nbox, c.xs, c.nb);
-    if (M.xs != c.xs || M.nb != c.nb) continue;  // does not fit
+    if (c.kern == 0 && (M.xs != c.xs || M.nb != c.nb)) continue;  // does not fit
     int rc = reset_outputs(ctx, st);
     if (rc) return rc;
     if ((rc = enqueue_multi(ctx, dx, sample, wpk, 0, st))) return rc;  // warm
@@ -198,13 +221,14 @@ int autotune(kg_ctx* ctx, const uint64_t* dx, uint64_t m, uint32_t wpk, cudaStre
     cudaEventElapsedTime(&ms, a, b);
     if (ms < best) {
       best = ms;
-      bxs = c.xs;
-      bnb = c.nb;
+      win = c;
     }
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
-  pick_shape(M, nbox, bxs, bnb);
+  M.kern = win.kern;
+  M.bt_scale = win.bt_scale;
+  pick_shape(M, nbox, win.xs, win.nb);
   M.tuned = true;
   M.tuned_nbox = nbox;
   return KG_OK;
@@ -300,6 +324,8 @@ int kg_set_phenotypes(kg_ctx* ctx, const kg_pheno* ph, int np, int n_row) {
   M.NP = NP;
   M.PPG = PPG;
   M.stationary = stationary;
+  M.pair_ok = stationary && PPG == 1 && np >= 2 && kg::mpb2_supported(NP, kpad, 16);
+  M.kern = stationary ? 1 : 0;
   M.G = G;
   M.kpad = kpad;
   // B image: group gi at gi*kpad*N in the make_b_image_ts layout (the
@@ -368,10 +394,10 @@ int kg_multi_shape(const kg_ctx* ctx, kg_tile_shape* out) {
   if (!ctx || !out) return KG_ERR_INVALID;
   const Multi& M = ctx->mp;
   if (M.np <= 0) return KG_ERR_STATE;
-  out->kernel = M.stationary ? 1 : 2;
+  out->kernel = M.kern == 2 ? 3 : M.kern == 1 ? 1 : 2;
   out->np = M.NP;
-  out->ppg = M.PPG;
-  out->groups = M.G;
+  out->ppg = M.kern == 2 ? 2 : M.PPG;
+  out->groups = M.kern == 2 ? (M.G + 1) / 2 : M.G;
   out->kpad = M.kpad;
   out->bt = M.bt;
   out->xs = M.xs;

@@ -66,6 +66,9 @@ struct Multi {
   int np = 0, n_row = 0, NP = 0, G = 0, kpad = 0, cm = 0, nsteps = 0;
   int PPG = 1;          // phenotypes per group (one MMA of NP * PPG columns)
   bool stationary = false;  // the group image fits in shared memory: kernel_mpb.cu
+  bool pair_ok = false;     // kernel_mpb2.cu can run these phenotypes (PPG = 1 images)
+  int kern = 0;             // chosen kernel: 0 image streamed (mp), 1 image resident (mpb), 2 SM pair (mpb2)
+  int bt_scale = 2;         // tile-iterations per L2 block: the 48 MB rule times bt_scale / 2
   int8_t* dB = nullptr;
   kg::MPheno* dPh = nullptr;
   double* dV = nullptr;

@@ -127,6 +127,15 @@ size_t mpb_smem_bytes(int N, int kpad);
 cudaError_t launch_mpb(const LaunchMpb& L, cudaStream_t st);
 cudaError_t launch_mp_refine(const LaunchMpRefine& L, cudaStream_t st);
 
+// Pair-of-SMs many-phenotype kernel (kernel_mpb2.cu): a cluster of two CTAs
+// issues M = 256 tcgen05 MMAs (cta_group::2) over two phenotypes at once
+// (N = 2 * NP), each CTA holding one phenotype's image (kpad x NP, the
+// one-phenotype-per-group image of LaunchMpb with PPG = 1; L.G = phenotypes)
+// and 128 k-mers of each 256-k-mer pair-tile.
+bool mpb2_supported(int NP, int kpad, int wpk);
+size_t mpb2_smem_bytes(int NP, int kpad);
+cudaError_t launch_mpb2(const LaunchMpb& L, cudaStream_t st);
+
 // 2-D pair test (kernel_pairs.cu): the TMEM-A pipeline on x_i AND x_j.
 struct LaunchPairs {
   const uint64_t* x;          // packed rows (device), 16-byte aligned, wpk >= 16

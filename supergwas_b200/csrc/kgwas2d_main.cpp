@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "../../include/kgwas_cuda.h"
+#include "cli.hpp"
 #include "kgwas_io.hpp"
 
 using kgio::die;
@@ -40,30 +41,37 @@ struct Config {  // src/kgwas_2d.cpp:24-35
   int device = 0;
 };
 
-static Config parse_args(int argc, char** argv) {  // src/kgwas_2d.cpp:45-78
-  if (argc < 6) {
-    std::cerr << "Usage: " << argv[0] << " samples.txt phenotype.txt U2D.bin INDEX_DIR out_prefix"
-              << " [log10_thresh] [--emit-threads N] [--out-chunk N]\n"
-              << "\nOutputs:\n"
-              << "  out_prefix.tsv   — idx_a, idx_b, effect, pvalue\n"
-              << "  out_prefix.kmers — one k-mer sequence per line (line# = index)\n";
-    std::exit(1);
-  }
+static void print_usage(const char* prog) {
+  std::cerr << "Usage: " << prog << " samples.txt phenotype.txt U2D.bin INDEX_DIR out_prefix"
+            << " [log10_thresh] [--emit-threads N] [--out-chunk N]\n"
+            << "\nOutputs:\n"
+            << "  out_prefix.tsv   — idx_a, idx_b, effect, pvalue\n"
+            << "  out_prefix.kmers — one k-mer sequence per line (line# = index)\n";
+}
+
+// The command line of src/kgwas_2d.cpp:44-76 as a table: five leading paths,
+// a -log10 threshold when the next word does not start with '-', then
+// integer options; other words are ignored.  Malformed numbers end the
+// program with an uncaught exception, as in the reference.
+static Config parse_args(int argc, char** argv) {
   Config cfg;
-  cfg.samples_file = argv[1];
-  cfg.pheno_file = argv[2];
-  cfg.U_file = argv[3];
-  cfg.index_dir = argv[4];
-  cfg.out_prefix = argv[5];
-  if (argc > 6 && argv[6][0] != '-') cfg.log10_thresh = std::stod(argv[6]);
-  const int start = (argc > 6 && argv[6][0] != '-') ? 7 : 6;
-  for (int i = start; i < argc; ++i) {
-    const string a = argv[i];
-    if (a == "--emit-threads" && i + 1 < argc) cfg.EMIT_THREADS = std::stoi(argv[++i]);
-    else if (a == "--out-chunk" && i + 1 < argc) cfg.OUT_CHUNK = std::stoi(argv[++i]);
-    else if (a == "--task-id" && i + 1 < argc) cfg.task_id = std::stoi(argv[++i]);
-    else if (a == "--num-tasks" && i + 1 < argc) cfg.num_tasks = std::stoi(argv[++i]);
-  }
+  kgcli::Grammar g;
+  g.required = 5;
+  g.usage = print_usage;
+  g.leading_accept = [](const string& w) { return w.empty() || w[0] != '-'; };
+  g.leading_take = [&](const string& w) { cfg.log10_thresh = std::stod(w); };
+  g.options = {
+      {"--emit-threads", [&](const string& v) { cfg.EMIT_THREADS = std::stoi(v); }},
+      {"--out-chunk", [&](const string& v) { cfg.OUT_CHUNK = std::stoi(v); }},
+      {"--task-id", [&](const string& v) { cfg.task_id = std::stoi(v); }},
+      {"--num-tasks", [&](const string& v) { cfg.num_tasks = std::stoi(v); }},
+  };
+  const vector<string> lead = kgcli::parse(argc, argv, g);
+  cfg.samples_file = lead[0];
+  cfg.pheno_file = lead[1];
+  cfg.U_file = lead[2];
+  cfg.index_dir = lead[3];
+  cfg.out_prefix = lead[4];
   cfg.BLAS_THREADS = kgio::env_int("BLAS_THREADS", cfg.BLAS_THREADS);
   cfg.EMIT_THREADS = kgio::env_int("EMIT_THREADS", cfg.EMIT_THREADS);
   if (const char* v = std::getenv("KGWAS_DEVICE")) cfg.device = std::atoi(v);

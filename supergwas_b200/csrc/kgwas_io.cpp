@@ -9,6 +9,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cerrno>
+#include <climits>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -38,14 +40,18 @@ void die(const std::string& m) {
 
 void warn(const std::string& m) { std::cerr << "[WARN] " << m << "\n"; }
 
-int env_int(const char* k, int dflt) {
-  const char* v = std::getenv(k);
-  if (!v || !*v) return dflt;
-  try {
-    return std::max(1, std::stoi(v));
-  } catch (...) {
-    return dflt;
-  }
+// A thread count from the environment: the leading integer of the value
+// (after blanks, with an optional sign; trailing text ignored), at least 1;
+// `fallback` when the variable is unset or empty, has no leading integer or
+// leaves the int range.
+int env_int(const char* name, int fallback) {
+  const char* text = std::getenv(name);
+  if (text == nullptr || text[0] == '\0') return fallback;
+  errno = 0;
+  char* stop = nullptr;
+  const long v = std::strtol(text, &stop, 10);
+  if (stop == text || errno == ERANGE || v < INT_MIN || v > INT_MAX) return fallback;
+  return v < 1 ? 1 : (int)v;
 }
 
 static double now_s() {
@@ -55,147 +61,337 @@ static double now_s() {
 Timer::Timer() : t0(now_s()) {}
 double Timer::sec() const { return now_s() - t0; }
 
-std::vector<std::string> load_lines(const std::string& file) {
-  std::ifstream in(file);
-  if (!in) die("open: " + file);
-  std::vector<std::string> v;
-  std::string s;
-  while (std::getline(in, s))
-    if (!s.empty()) {
-      if (s.back() == '\r') s.pop_back();
-      v.push_back(s);
+// ------------------------------------------------------------ input sources
+namespace {
+
+// A regular file mapped read-only for the lifetime of the object.  open()
+// reports which step failed; files shorter than `min_size` are not mapped.
+class MappedFile {
+ public:
+  enum Status { kOk, kEmpty, kTooShort, kNotRegular, kOpenFailed, kStatFailed, kMapFailed };
+  MappedFile() = default;
+  MappedFile(const MappedFile&) = delete;
+  MappedFile& operator=(const MappedFile&) = delete;
+  MappedFile(MappedFile&& o) noexcept { swap(o); }
+  MappedFile& operator=(MappedFile&& o) noexcept {
+    swap(o);
+    return *this;
+  }
+  ~MappedFile() {
+    if (base_) munmap(base_, size_);
+  }
+
+  Status open(const std::string& path, size_t min_size = 1) {
+    const int fd = ::open(path.c_str(), O_RDONLY);
+    if (fd < 0) return kOpenFailed;
+    struct stat info {};
+    Status s = kOk;
+    if (fstat(fd, &info) != 0) s = kStatFailed;
+    else if (!S_ISREG(info.st_mode)) s = kNotRegular;
+    else {
+      size_ = (size_t)info.st_size;
+      if (size_ == 0) s = kEmpty;
+      else if (size_ < min_size) s = kTooShort;
+      else {
+        void* p = mmap(nullptr, size_, PROT_READ, MAP_PRIVATE, fd, 0);
+        if (p == MAP_FAILED) s = kMapFailed;
+        else {
+          base_ = p;
+          madvise(p, size_, MADV_SEQUENTIAL);
+        }
+      }
     }
-  return v;
+    ::close(fd);
+    return s;
+  }
+  const unsigned char* bytes() const { return static_cast<const unsigned char*>(base_); }
+  size_t size() const { return size_; }
+
+ private:
+  void swap(MappedFile& o) noexcept {
+    std::swap(base_, o.base_);
+    std::swap(size_, o.size_);
+  }
+  void* base_ = nullptr;
+  size_t size_ = 0;
+};
+
+// A gzip stream read through zlib's gz interface with a 1 MB buffer.
+class GzSource {
+ public:
+  explicit GzSource(const std::string& path) : f_(gzopen(path.c_str(), "rb")) {
+    if (f_) gzbuffer(f_, 1u << 20);
+  }
+  GzSource(const GzSource&) = delete;
+  GzSource& operator=(const GzSource&) = delete;
+  ~GzSource() {
+    if (f_) gzclose(f_);
+  }
+  bool ok() const { return f_ != nullptr; }
+  // Up to `len` inflated bytes (fewer only at the end of the stream); -1 when
+  // zlib reports an error (see error()).
+  long long fill(void* dst, size_t len) {
+    size_t have = 0;
+    while (have < len) {
+      const unsigned ask = (unsigned)std::min<size_t>(len - have, (size_t)1 << 30);
+      const int r = gzread(f_, static_cast<unsigned char*>(dst) + have, ask);
+      if (r < 0) return -1;
+      if (r == 0) break;
+      have += (size_t)r;
+    }
+    return (long long)have;
+  }
+  // zlib's state after a short or failed fill: its message and code.
+  std::string error(int* code = nullptr) const {
+    int c = Z_OK;
+    const char* m = gzerror(f_, &c);
+    if (code) *code = c;
+    return m ? m : "";
+  }
+
+ private:
+  gzFile f_;
+};
+
+// Whole file as bytes; false when it cannot be opened.
+bool slurp(const std::string& path, std::string& out) {
+  std::FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) return false;
+  out.clear();
+  char chunk[1 << 16];
+  size_t got;
+  while ((got = std::fread(chunk, 1, sizeof(chunk), f)) > 0) out.append(chunk, got);
+  std::fclose(f);
+  return true;
 }
 
-std::unordered_map<std::string, double> load_pheno(const std::string& file) {
-  std::ifstream in(file);
-  if (!in) die("open: " + file);
-  std::unordered_map<std::string, double> m;
+// Calls fn(begin, length) for each '\n'-terminated line of [p, p + len) and
+// for a last line without '\n' when it is not empty (std::getline's lines).
+template <class Fn>
+void for_each_line(const char* p, size_t len, Fn&& fn) {
+  const char* end = p + len;
+  while (p < end) {
+    const char* nl = static_cast<const char*>(std::memchr(p, '\n', (size_t)(end - p)));
+    const char* stop = nl ? nl : end;
+    fn(p, (size_t)(stop - p));
+    if (!nl) break;
+    p = nl + 1;
+  }
+}
+
+bool is_regular(const std::string& p) {
+  struct stat info {};
+  return ::stat(p.c_str(), &info) == 0 && S_ISREG(info.st_mode);
+}
+
+// Where the column of one sample lives: bits/col_%06d.txt, else the same
+// name with .gz (src/kgwas_utils.hpp:238-240).
+struct ColumnFile {
+  std::string plain, gz;
+  enum Kind { kPlain, kGz, kMissing } kind;
+};
+ColumnFile locate_column(const std::string& bits_dir, int sample_pos) {
+  char name[48];
+  std::snprintf(name, sizeof(name), "/col_%06d.txt", sample_pos);
+  ColumnFile c;
+  c.plain = bits_dir + name;
+  c.gz = c.plain + ".gz";
+  c.kind = is_regular(c.plain) ? ColumnFile::kPlain : is_regular(c.gz) ? ColumnFile::kGz : ColumnFile::kMissing;
+  return c;
+}
+[[noreturn]] void die_missing(const ColumnFile& c) { die("missing column: " + c.plain + " (and " + c.gz + ")"); }
+
+// Length of the first line of a column file: the bytes before the first
+// '\n', or the whole file when it has none.
+size_t first_line_plain(const std::string& path) {
+  MappedFile f;
+  switch (f.open(path)) {
+    case MappedFile::kOpenFailed: die("open: " + path);
+    case MappedFile::kStatFailed: die("fstat: " + path);
+    case MappedFile::kEmpty: die("empty: " + path);
+    case MappedFile::kMapFailed:
+    case MappedFile::kNotRegular:
+    case MappedFile::kTooShort: die("mmap: " + path);
+    case MappedFile::kOk: break;
+  }
+  const void* nl = std::memchr(f.bytes(), '\n', f.size());
+  const size_t len = nl ? (size_t)(static_cast<const unsigned char*>(nl) - f.bytes()) : f.size();
+  if (len == 0) die("no bytes before newline: " + path);
+  return len;
+}
+
+size_t first_line_gz(const std::string& path) {
+  GzSource z(path);
+  if (!z.ok()) die("gzopen: " + path);
+  std::vector<unsigned char> block((size_t)1 << 20);
+  size_t before = 0;  // bytes of the first line in earlier blocks
+  for (;;) {
+    const long long got = z.fill(block.data(), block.size());
+    if (got < 0) die("gzread error: " + z.error());
+    const void* nl = std::memchr(block.data(), '\n', (size_t)got);
+    if (nl) return before + (size_t)(static_cast<const unsigned char*>(nl) - block.data());
+    before += (size_t)got;
+    if ((size_t)got < block.size()) break;  // end of stream
+  }
+  if (before == 0) die("empty gz column: " + path);
+  return before;
+}
+
+// One sample's column of N bytes: a mapping of the plain file, or the first
+// N inflated bytes of the .gz file, which must end there or with '\n'.
+struct ColumnBytes {
+  MappedFile map;
+  std::unique_ptr<unsigned char[]> inflated;
+  const unsigned char* p = nullptr;
+};
+
+void open_column(const ColumnFile& c, size_t N, ColumnBytes& out) {
+  if (c.kind == ColumnFile::kMissing) die_missing(c);
+  if (c.kind == ColumnFile::kPlain) {
+    switch (out.map.open(c.plain, N)) {
+      case MappedFile::kOpenFailed: die("open: " + c.plain);
+      case MappedFile::kStatFailed: die("fstat: " + c.plain);
+      case MappedFile::kEmpty:
+      case MappedFile::kTooShort:
+        die("short column: " + c.plain + " (size " + std::to_string(out.map.size()) + " < N " + std::to_string(N) +
+            ")");
+      case MappedFile::kNotRegular:
+      case MappedFile::kMapFailed: die("mmap: " + c.plain);
+      case MappedFile::kOk: break;
+    }
+    out.p = out.map.bytes();
+    return;
+  }
+  GzSource z(c.gz);
+  if (!z.ok()) die("gzopen: " + c.gz);
+  out.inflated.reset(new unsigned char[N + 1]);
+  const long long got = z.fill(out.inflated.get(), N);
+  if (got < 0 || (size_t)got < N) {
+    int code = Z_OK;
+    const std::string msg = z.error(&code);
+    if (got >= 0 && code == Z_STREAM_END)
+      die("short gz column: " + c.gz + " (got " + std::to_string(got) + " < N " + std::to_string(N) + ")");
+    die("gzread error: " + msg);
+  }
+  // one byte past the column may only be the line end
+  if (z.fill(out.inflated.get() + N, 1) == 1 && out.inflated[N] != '\n')
+    die("gz column longer than expected (N+ extra non-newline): " + c.gz);
+  out.p = out.inflated.get();
+}
+
+}  // namespace
+
+// ---------------------------------------------------- samples and phenotype
+std::vector<std::string> read_sample_ids(const std::string& file) {
+  std::string text;
+  if (!slurp(file, text)) die("open: " + file);
+  std::vector<std::string> ids;
+  for_each_line(text.data(), text.size(), [&](const char* p, size_t len) {
+    if (len == 0) return;                   // empty lines are skipped ...
+    if (p[len - 1] == '\r') --len;          // ... before one '\r' is dropped
+    ids.emplace_back(p, len);
+  });
+  return ids;
+}
+
+// The phenotype file is a sequence of whitespace-separated (id, value) pairs
+// read with formatted stream extraction, up to the first pair that does not
+// parse; a later pair for the same id replaces an earlier one.  Each value
+// goes to every position of its id in the sample list.
+Overlap match_phenotypes(const std::vector<std::string>& ids, const std::string& pheno_file) {
+  std::unordered_map<std::string, std::vector<int>> positions;
+  positions.reserve(ids.size());
+  for (int j = 0; j < (int)ids.size(); ++j) positions[ids[j]].push_back(j);
+  std::string text;
+  if (!slurp(pheno_file, text)) die("open: " + pheno_file);
+  std::vector<double> value(ids.size(), 0.0);
+  std::vector<char> seen(ids.size(), 0);
+  std::istringstream pairs(std::move(text));
   std::string id;
-  double val;
-  while (in >> id >> val) m[id] = val;
-  return m;
+  double v = 0.0;
+  while (pairs >> id >> v) {
+    const auto hit = positions.find(id);
+    if (hit == positions.end()) continue;
+    for (int j : hit->second) {
+      value[j] = v;
+      seen[j] = 1;
+    }
+  }
+  Overlap ov;
+  for (int j = 0; j < (int)ids.size(); ++j)
+    if (seen[j]) {
+      ov.idxs.push_back(j);
+      ov.y.push_back(value[j]);
+    }
+  ov.samples = ids;
+  return ov;
 }
 
 Overlap build_overlap(const std::string& samples_file, const std::string& pheno_file) {
   Timer t;
-  Overlap ov;
-  ov.samples = load_lines(samples_file);
-  const int L = (int)ov.samples.size();
-  if (L <= 0) die("samples empty");
-  auto ph = load_pheno(pheno_file);
-  for (int j = 0; j < L; ++j) {
-    auto it = ph.find(ov.samples[j]);
-    if (it != ph.end()) {
-      ov.idxs.push_back(j);
-      ov.y.push_back(it->second);
-    }
-  }
+  const std::vector<std::string> ids = read_sample_ids(samples_file);
+  if (ids.empty()) die("samples empty");
+  Overlap ov = match_phenotypes(ids, pheno_file);
   if (ov.idxs.empty()) die("no phenotype overlap");
   std::cerr << "[INFO] n=" << ov.y.size() << " (overlap)  (" << t.sec() << " s)\n";
   return ov;
 }
 
+// -------------------------------------------------------------------- U.bin
+UbinFile read_ubin_file(const std::string& path) {
+  UbinFile u;
+  std::string bytes;
+  if (!slurp(path, bytes)) {
+    u.status = UbinFile::kNoFile;
+    return u;
+  }
+  int32_t head[2] = {0, 0};
+  std::memcpy(head, bytes.data(), std::min<size_t>(bytes.size(), sizeof(head)));
+  u.n = head[0];
+  u.k = head[1];
+  u.header_bytes = std::min<size_t>(bytes.size(), sizeof(head));
+  if (u.header_bytes < sizeof(head)) {
+    u.status = UbinFile::kShortHeader;
+    return u;
+  }
+  const size_t body = bytes.size() - sizeof(head);
+  if (u.n < 0 || u.k < 0) {
+    u.status = UbinFile::kShortBody;
+    return u;
+  }
+  const size_t want = (size_t)u.n * (size_t)u.k;
+  const size_t have = std::min(want, body / sizeof(double));
+  u.U.resize(have);
+  if (have) std::memcpy(u.U.data(), bytes.data() + sizeof(head), have * sizeof(double));
+  u.status = have == want ? UbinFile::kOk : UbinFile::kShortBody;
+  return u;
+}
+
 UData load_ubin(const std::string& path, int n) {
   Timer t;
-  std::ifstream uin(path, std::ios::binary);
-  if (!uin) die("open: " + path);
-  int n_u = 0, r = 0;
-  uin.read((char*)&n_u, sizeof(int));
-  uin.read((char*)&r, sizeof(int));
-  if (!uin) die("short U.bin header");
-  if (n_u != n) die("U.bin n mismatch: file n=" + std::to_string(n_u) + " vs overlap n=" + std::to_string(n));
-  if (r < 0) die("short U.bin body");
+  UbinFile f = read_ubin_file(path);
+  if (f.status == UbinFile::kNoFile) die("open: " + path);
+  if (f.status == UbinFile::kShortHeader) die("short U.bin header");
+  if (f.n != n) die("U.bin n mismatch: file n=" + std::to_string(f.n) + " vs overlap n=" + std::to_string(n));
+  if (f.status != UbinFile::kOk) die("short U.bin body");
   UData ud;
   ud.n = n;
-  ud.k = r;
-  ud.U.resize((size_t)n * r);
-  uin.read((char*)ud.U.data(), (std::streamsize)(sizeof(double) * (size_t)n * r));
-  if (!uin) die("short U.bin body");
-  std::cerr << "[INFO] loaded U (n=" << n << ", r=" << r << ")  (" << t.sec() << " s)\n";
+  ud.k = f.k;
+  ud.U = std::move(f.U);
+  std::cerr << "[INFO] loaded U (n=" << n << ", r=" << ud.k << ")  (" << t.sec() << " s)\n";
   return ud;
 }
 
-static bool file_exists(const std::string& p) {
-  struct stat st {};
-  return ::stat(p.c_str(), &st) == 0 && S_ISREG(st.st_mode);
-}
-
-static size_t probe_N_txt(const std::string& path) {
-  int fd = ::open(path.c_str(), O_RDONLY);
-  if (fd < 0) die("open: " + path);
-  struct stat st {};
-  if (fstat(fd, &st) != 0) {
-    ::close(fd);
-    die("fstat: " + path);
-  }
-  const size_t sz = (size_t)st.st_size;
-  if (sz == 0) {
-    ::close(fd);
-    die("empty: " + path);
-  }
-  void* p = mmap(nullptr, sz, PROT_READ, MAP_PRIVATE, fd, 0);
-  if (p == MAP_FAILED) {
-    ::close(fd);
-    die("mmap: " + path);
-  }
-  const char* b = (const char*)p;
-  const void* nl = memchr(b, '\n', sz);
-  const size_t N = nl ? (size_t)((const char*)nl - b) : sz;
-  munmap(p, sz);
-  ::close(fd);
-  if (N == 0) die("no bytes before newline: " + path);
-  return N;
-}
-
-static size_t probe_N_gz(const std::string& path) {
-  gzFile f = gzopen(path.c_str(), "rb");
-  if (!f) die("gzopen: " + path);
-  gzbuffer(f, 1 << 20);
-  const size_t CHUNK = 1 << 20;
-  std::unique_ptr<unsigned char[]> buf(new unsigned char[CHUNK]);
-  size_t total = 0;
-  for (;;) {
-    int n = gzread(f, buf.get(), (unsigned)CHUNK);
-    if (n < 0) {
-      int err = 0;
-      const char* msg = gzerror(f, &err);
-      gzclose(f);
-      die(std::string("gzread error: ") + (msg ? msg : ""));
-    }
-    if (n == 0) break;
-    const void* nl = memchr(buf.get(), '\n', (size_t)n);
-    if (nl) {
-      total += (size_t)((const unsigned char*)nl - buf.get());
-      gzclose(f);
-      return total;
-    }
-    total += (size_t)n;
-  }
-  gzclose(f);
-  if (total == 0) die("empty gz column: " + path);
-  return total;
-}
-
-static std::string col_name(int idx) {
-  char base[64];
-  std::snprintf(base, sizeof(base), "col_%06d.txt", idx);
-  return base;
-}
-
+// ---------------------------------------------------------- batch directory
 size_t infer_N_from_bits(const std::string& bits_dir, int first_idx) {
   Timer t;
-  const std::string p_txt = bits_dir + "/" + col_name(first_idx);
-  const std::string p_gz = p_txt + ".gz";
-  size_t N = 0;
-  const bool txt = file_exists(p_txt);
-  if (txt) N = probe_N_txt(p_txt);
-  else if (file_exists(p_gz)) N = probe_N_gz(p_gz);
-  else die("missing column: " + p_txt + " (and " + p_gz + ")");
+  const ColumnFile c = locate_column(bits_dir, first_idx);
+  if (c.kind == ColumnFile::kMissing) die_missing(c);
+  const bool plain = c.kind == ColumnFile::kPlain;
+  const size_t N = plain ? first_line_plain(c.plain) : first_line_gz(c.gz);
   if (N == 0) die("N=0");
-  std::cerr << "[INFO] inferred N=" << N << " rows  (" << t.sec() << " s)" << (txt ? " [from .txt]" : " [from .txt.gz]")
-            << "\n";
+  std::cerr << "[INFO] inferred N=" << N << " rows  (" << t.sec() << " s)"
+            << (plain ? " [from .txt]" : " [from .txt.gz]") << "\n";
   return N;
 }
 
@@ -204,23 +400,18 @@ std::vector<std::string> load_kmers(const std::string& path, size_t N) {
   kmers.reserve(N);
   const bool gz = path.size() >= 3 && path.compare(path.size() - 3, 3, ".gz") == 0;
   if (gz) {
-    gzFile f = gzopen(path.c_str(), "rb");
-    if (!f) die("gzopen: " + path);
-    gzbuffer(f, 1u << 20);
+    GzSource z(path);
+    if (!z.ok()) die("gzopen: " + path);
     // inflated in 4 MB blocks and split at '\n'; only '\n'-terminated lines
     // count (an unterminated last line is not a k-mer), as with gzgets
     std::vector<char> buf((size_t)4 << 20);
     std::string part;  // a line that continues in the next block
     while (kmers.size() < N) {
-      const int r = gzread(f, buf.data(), (unsigned)buf.size());
+      const long long r = z.fill(buf.data(), buf.size());
       if (r <= 0) {
-        int err = 0;
-        const char* msg = gzerror(f, &err);
-        if (r < 0 || (err != Z_OK && err != Z_STREAM_END)) {
-          const std::string m = msg ? msg : "";
-          gzclose(f);
-          die("gzgets error: " + m);
-        }
+        int code = Z_OK;
+        const std::string msg = z.error(&code);
+        if (r < 0 || (code != Z_OK && code != Z_STREAM_END)) die("gzgets error: " + msg);
         break;
       }
       const char* p = buf.data();
@@ -241,14 +432,19 @@ std::vector<std::string> load_kmers(const std::string& path, size_t N) {
         p = nl + 1;
       }
     }
-    gzclose(f);
   } else {
-    std::ifstream in(path);
-    if (!in) die("open: " + path);
-    std::string s;
-    while (kmers.size() < N && std::getline(in, s)) {
-      if (!s.empty() && s.back() == '\r') s.pop_back();
-      kmers.push_back(std::move(s));
+    // plain: std::getline's lines (a last line without '\n' counts), one
+    // trailing '\r' dropped, empty lines kept
+    MappedFile f;
+    const MappedFile::Status s = f.open(path);
+    if (s == MappedFile::kOpenFailed) die("open: " + path);
+    if (s == MappedFile::kOk) {
+      const char* text = reinterpret_cast<const char*>(f.bytes());
+      for_each_line(text, f.size(), [&](const char* p, size_t len) {
+        if (kmers.size() >= N) return;
+        if (len && p[len - 1] == '\r') --len;
+        kmers.emplace_back(p, len);
+      });
     }
   }
   if (kmers.size() != N)
@@ -256,81 +452,17 @@ std::vector<std::string> load_kmers(const std::string& path, size_t N) {
   return kmers;
 }
 
-static void read_gz_exact_N(const std::string& path, unsigned char* dst, size_t N) {
-  gzFile f = gzopen(path.c_str(), "rb");
-  if (!f) die("gzopen: " + path);
-  gzbuffer(f, 1 << 20);
-  size_t got = 0;
-  while (got < N) {
-    int n = gzread(f, dst + got, (unsigned)std::min<size_t>(N - got, 1 << 20));
-    if (n <= 0) {
-      int err = 0;
-      const char* msg = gzerror(f, &err);
-      gzclose(f);
-      if (err == Z_STREAM_END)
-        die("short gz column: " + path + " (got " + std::to_string(got) + " < N " + std::to_string(N) + ")");
-      die(std::string("gzread error: ") + (msg ? msg : ""));
-    }
-    got += (size_t)n;
-  }
-  unsigned char extra;
-  int n = gzread(f, &extra, 1);
-  if (n == 1 && extra != '\n') {
-    gzclose(f);
-    die("gz column longer than expected (N+ extra non-newline): " + path);
-  }
-  gzclose(f);
-}
-
-namespace {
-struct Column {
-  const unsigned char* p = nullptr;
-  void* map = nullptr;
-  size_t map_sz = 0;
-  std::unique_ptr<unsigned char[]> buf;
-};
-}  // namespace
-
 void load_matrix_packed(const std::string& bits_dir, const std::vector<int>& idxs, size_t N, int threads,
                         uint64_t* out) {
   Timer t;
   const int n = (int)idxs.size();
   const uint32_t W = words_per_kmer(n);
-  std::vector<Column> cols(n);
+  std::vector<ColumnBytes> cols(n);
   std::atomic<int> done{0};
   omp_set_num_threads(std::max(1, threads));
 #pragma omp parallel for schedule(dynamic, 1)
   for (int k = 0; k < n; ++k) {
-    const std::string p_txt = bits_dir + "/" + col_name(idxs[k]);
-    const std::string p_gz = p_txt + ".gz";
-    Column& c = cols[k];
-    if (file_exists(p_txt)) {
-      int fd = ::open(p_txt.c_str(), O_RDONLY);
-      if (fd < 0) die("open: " + p_txt);
-      struct stat st {};
-      if (fstat(fd, &st) != 0) {
-        ::close(fd);
-        die("fstat: " + p_txt);
-      }
-      const size_t sz = (size_t)st.st_size;
-      if (sz < N) {
-        ::close(fd);
-        die("short column: " + p_txt + " (size " + std::to_string(sz) + " < N " + std::to_string(N) + ")");
-      }
-      void* p = mmap(nullptr, sz, PROT_READ, MAP_PRIVATE, fd, 0);
-      ::close(fd);
-      if (p == MAP_FAILED) die("mmap: " + p_txt);
-      madvise(p, sz, MADV_SEQUENTIAL);
-      c.map = p;
-      c.map_sz = sz;
-      c.p = (const unsigned char*)p;
-    } else if (file_exists(p_gz)) {
-      c.buf.reset(new unsigned char[N]);
-      read_gz_exact_N(p_gz, c.buf.get(), N);
-      c.p = c.buf.get();
-    } else {
-      die("missing column: " + p_txt + " (and " + p_gz + ")");
-    }
+    open_column(locate_column(bits_dir, idxs[k]), N, cols[k]);
     const int d = ++done;
     if ((d % 8) == 0) {
 #pragma omp critical
@@ -377,8 +509,6 @@ void load_matrix_packed(const std::string& bits_dir, const std::vector<int>& idx
       }
     }
   }
-  for (auto& c : cols)
-    if (c.map) munmap(c.map, c.map_sz);
   std::cerr << "\r[LOAD] " << n << "/" << n << "  (" << t.sec() << " s, LOAD_THREADS=" << threads << ")\n";
 }
 

@@ -13,7 +13,10 @@ namespace kgio {
 
 [[noreturn]] void die(const std::string& m);   // "[ERROR] m", exit(1)
 void warn(const std::string& m);               // "[WARN] m"
-int env_int(const char* k, int dflt);          // src/kgwas_utils.hpp:43-47
+// Thread counts from the environment (LOAD_THREADS, BLAS_THREADS,
+// EMIT_THREADS; src/kgwas_utils.hpp:43-47): the leading integer, at least 1,
+// else `fallback`.
+int env_int(const char* name, int fallback);
 
 struct Timer {
   double t0;
@@ -21,26 +24,43 @@ struct Timer {
   double sec() const;
 };
 
-// src/kgwas_utils.hpp:51-61: skip empty lines, drop one trailing '\r'.
-std::vector<std::string> load_lines(const std::string& file);
-// src/kgwas_utils.hpp:63-70: whitespace-separated "id value"; last duplicate wins.
-std::unordered_map<std::string, double> load_pheno(const std::string& file);
+// samples.txt (src/kgwas_utils.hpp:51-61): one id per line, empty lines
+// skipped, one trailing '\r' dropped.  "[ERROR] open: file" when unreadable.
+std::vector<std::string> read_sample_ids(const std::string& file);
 
-struct Overlap {                                // src/kgwas_utils.hpp:285-314
+// The overlap of the sample list with a phenotype file of whitespace-
+// separated "id value" pairs (src/kgwas_utils.hpp:63-70, 285-314): the
+// positions in the sample list whose id has a value, in list order, and
+// their values (the last pair of an id wins).  No emptiness checks.
+struct Overlap {
   std::vector<int> idxs;                        // positions in samples.txt
   std::vector<std::string> samples;
   std::vector<double> y;
 };
+Overlap match_phenotypes(const std::vector<std::string>& ids, const std::string& pheno_file);
+// COLS mode: read_sample_ids + match_phenotypes with the "samples empty" and
+// "no phenotype overlap" checks and the [INFO] line.
 Overlap build_overlap(const std::string& samples_file, const std::string& pheno_file);
 
-struct UData {                                  // src/kgwas_utils.hpp:129-157
+// U.bin (src/compute_structure_all.cpp:80-88): int32 n, int32 k, then n*k
+// FP64 column-major.  read_ubin_file only parses; the modes word their own
+// errors (COLS: load_ubin, src/kgwas_utils.hpp:129-157; ROWS:
+// src/kgwas.cpp:372-381).
+struct UbinFile {
+  enum Status { kOk, kNoFile, kShortHeader, kShortBody } status = kNoFile;
+  int n = 0, k = 0;           // header fields that were present (0 otherwise)
+  size_t header_bytes = 0;
+  std::vector<double> U;      // the values present: n*k when the body is complete
+};
+UbinFile read_ubin_file(const std::string& path);
+struct UData {
   std::vector<double> U;                        // n x k column-major
   int n = 0, k = 0;
 };
 UData load_ubin(const std::string& path, int n);
 
-size_t infer_N_from_bits(const std::string& bits_dir, int first_idx);   // :317-332
-std::vector<std::string> load_kmers(const std::string& path, size_t N);  // :93-127
+size_t infer_N_from_bits(const std::string& bits_dir, int first_idx);   // src/kgwas_utils.hpp:317-332
+std::vector<std::string> load_kmers(const std::string& path, size_t N);  // src/kgwas_utils.hpp:93-127
 
 inline uint32_t words_per_kmer(int n) {
   uint32_t w = (uint32_t)((n + 63) / 64);

@@ -30,6 +30,7 @@
 #include <memory>
 #include <thread>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -39,6 +40,7 @@
 #include <vector>
 
 #include "../../include/kgwas_cuda.h"
+#include "cli.hpp"
 #include "kgwas_io.hpp"
 
 using kgio::die;
@@ -62,67 +64,69 @@ struct Config {                      // src/kgwas.cpp:26-35
   uint32_t index_2d_shards = 4;  // build_index_2d.sh's
 };
 
-static Config parse_args(int argc, char** argv) {  // src/kgwas.cpp:67-126
-  if (argc < 6) {
-    std::cerr << "Usage: " << argv[0]
-              << " samples.txt phenotype.txt INPUT U.bin output.tsv [log10_thresh] [--mode cols|rows]\n"
-              << "\n"
-              << "  INPUT: directory (batch with bits/ + kmers.txt.gz) for COLS mode,\n"
-              << "         or a .tsv[.gz] file for ROWS mode.\n"
-              << "  Auto-detects mode from INPUT type unless --mode is specified.\n"
-              << "\n"
-              << "  Index outputs: --index-out DIR [--index-shards M] (the .tsv rows),\n"
-              << "                 --index-2d-out DIR [--index-2d-shards M] (the .2d rows)\n"
-              << "\n"
-              << "  Env: LOAD_THREADS, BLAS_THREADS, EMIT_THREADS, CORR_THRESHOLD, BATCH_SIZE,\n"
-              << "       KGWAS_PRECISION (split|fp64), KGWAS_DEVICE\n";
-    std::exit(1);
-  }
+static void print_usage(const char* prog) {
+  std::cerr << "Usage: " << prog
+            << " samples.txt phenotype.txt INPUT U.bin output.tsv [log10_thresh] [--mode cols|rows]\n"
+            << "\n"
+            << "  INPUT: directory (batch with bits/ + kmers.txt.gz) for COLS mode,\n"
+            << "         or a .tsv[.gz] file for ROWS mode.\n"
+            << "  Auto-detects mode from INPUT type unless --mode is specified.\n"
+            << "\n"
+            << "  Index outputs: --index-out DIR [--index-shards M] (the .tsv rows),\n"
+            << "                 --index-2d-out DIR [--index-2d-shards M] (the .2d rows)\n"
+            << "\n"
+            << "  Env: LOAD_THREADS, BLAS_THREADS, EMIT_THREADS, CORR_THRESHOLD, BATCH_SIZE,\n"
+            << "       KGWAS_PRECISION (split|fp64), KGWAS_DEVICE\n";
+}
+
+// The command line of src/kgwas.cpp:67-126 as a table: five leading paths,
+// then options and -log10 thresholds (a later threshold replaces an earlier
+// one; a word that is no number is an error).
+static Config parse_args(int argc, char** argv) {
   Config cfg;
-  cfg.samples_file = argv[1];
-  cfg.pheno_file = argv[2];
-  cfg.input_path = argv[3];
-  cfg.U_file = argv[4];
-  cfg.out_file = argv[5];
-  for (int i = 6; i < argc; ++i) {
-    string a = argv[i];
-    if (a == "--mode" && i + 1 < argc) {
-      cfg.mode = argv[++i];
-    } else if (a == "--log10-thresh-2d" && i + 1 < argc) {
-      cfg.log10_thresh_2d = std::stod(argv[++i]);
-    } else if (a == "--index-out" && i + 1 < argc) {
-      cfg.index_out = argv[++i];
-    } else if (a == "--index-shards" && i + 1 < argc) {
-      cfg.index_shards = (uint32_t)std::stoul(argv[++i]);
-    } else if (a == "--index-2d-out" && i + 1 < argc) {
-      cfg.index_2d_out = argv[++i];
-    } else if (a == "--index-2d-shards" && i + 1 < argc) {
-      cfg.index_2d_shards = (uint32_t)std::stoul(argv[++i]);
-    } else {
-      try {
-        cfg.log10_thresh = std::stod(a);
-      } catch (...) {
-        die("invalid argument: " + a);
-      }
-      if (cfg.log10_thresh < 0.0) die("threshold must be >= 0");
+  kgcli::Grammar g;
+  g.required = 5;
+  g.usage = print_usage;
+  g.options = {
+      {"--mode", [&](const string& v) { cfg.mode = v; }},
+      {"--log10-thresh-2d", [&](const string& v) { cfg.log10_thresh_2d = std::stod(v); }},
+      {"--index-out", [&](const string& v) { cfg.index_out = v; }},
+      {"--index-shards", [&](const string& v) { cfg.index_shards = (uint32_t)std::stoul(v); }},
+      {"--index-2d-out", [&](const string& v) { cfg.index_2d_out = v; }},
+      {"--index-2d-shards", [&](const string& v) { cfg.index_2d_shards = (uint32_t)std::stoul(v); }},
+  };
+  g.other = [&](const string& w) {
+    double t = 0.0;
+    try {
+      t = std::stod(w);
+    } catch (...) {
+      die("invalid argument: " + w);
     }
-  }
+    if (t < 0.0) die("threshold must be >= 0");
+    cfg.log10_thresh = t;
+  };
+  const vector<string> lead = kgcli::parse(argc, argv, g);
+  cfg.samples_file = lead[0];
+  cfg.pheno_file = lead[1];
+  cfg.input_path = lead[2];
+  cfg.U_file = lead[3];
+  cfg.out_file = lead[4];
   cfg.LOAD_THREADS = kgio::env_int("LOAD_THREADS", cfg.LOAD_THREADS);
   cfg.BLAS_THREADS = kgio::env_int("BLAS_THREADS", cfg.BLAS_THREADS);
   cfg.EMIT_THREADS = kgio::env_int("EMIT_THREADS", cfg.EMIT_THREADS);
   if (const char* v = std::getenv("CORR_THRESHOLD")) cfg.corr_threshold = std::stod(v);
   if (const char* v = std::getenv("LOG10_THRESH_2D_INPUT")) cfg.log10_thresh_2d = std::stod(v);
   if (const char* v = std::getenv("KGWAS_PRECISION")) {
-    string p = v;
+    const string p = v;
     if (p == "fp64") cfg.precision = KG_PREC_FP64;
     else if (p == "split" || p.empty()) cfg.precision = KG_PREC_SPLIT_I8;
     else die("KGWAS_PRECISION must be 'split' or 'fp64', got: " + p);
   }
   if (const char* v = std::getenv("KGWAS_DEVICE")) cfg.device = std::atoi(v);
-  if (cfg.mode.empty()) {
-    struct stat st {};
-    if (::stat(cfg.input_path.c_str(), &st) != 0) die("cannot stat INPUT: " + cfg.input_path);
-    cfg.mode = S_ISDIR(st.st_mode) ? "cols" : "rows";
+  if (cfg.mode.empty()) {  // a directory is a COLS batch, anything else a ROWS file
+    struct stat info {};
+    if (::stat(cfg.input_path.c_str(), &info) != 0) die("cannot stat INPUT: " + cfg.input_path);
+    cfg.mode = S_ISDIR(info.st_mode) ? "cols" : "rows";
     std::cerr << "[INFO] auto-detected mode: " << cfg.mode << "\n";
   }
   if (cfg.mode != "cols" && cfg.mode != "rows") die("--mode must be 'cols' or 'rows', got: " + cfg.mode);
@@ -179,25 +183,31 @@ struct HostWords {
   }
 };
 
-static string path_2d(const string& out_file) {  // src/kgwas.cpp:273-278
+// The .2d.tsv path: ".2d" goes in front of the last '.' of the output path
+// (wherever that dot is), or at the end when there is none
+// (src/kgwas.cpp:273-278).
+static string path_2d(const string& out_file) {
   string p = out_file;
-  size_t dot = p.rfind('.');
-  if (dot != string::npos) return p.substr(0, dot) + ".2d" + p.substr(dot);
-  return p + ".2d";
+  const size_t dot = p.rfind('.');
+  p.insert(dot == string::npos ? p.size() : dot, ".2d");
+  return p;
 }
 
-static void write_count(const string& out_file, uint64_t n_tested) {  // src/kgwas.cpp:291-304
-  std::string countfile = out_file + ".count";
-  std::string shardname = out_file;
-  size_t lastslash = shardname.find_last_of("/\\");
-  if (lastslash != std::string::npos) shardname = shardname.substr(lastslash + 1);
-  size_t lastdot = shardname.find_last_of('.');
-  if (lastdot != std::string::npos) shardname = shardname.substr(0, lastdot);
-  std::ofstream countout(countfile);
-  if (countout.is_open()) {
-    countout << shardname << "\t" << n_tested << "\n";
-    std::cerr << "[INFO] Count written to " << countfile << "\n";
-  }
+// The .count file (src/kgwas.cpp:291-304): "<label>\t<tested>\n" in
+// out_file + ".count", the label being the output file's name without its
+// directory ('/' or '\\') and without its last extension.  Nothing is written
+// when the file cannot be created.
+static void write_count(const string& out_file, uint64_t n_tested) {
+  const size_t name_at = out_file.find_last_of("/\\");
+  string label = name_at == string::npos ? out_file : out_file.substr(name_at + 1);
+  const size_t ext = label.find_last_of('.');
+  if (ext != string::npos) label.erase(ext);
+  const string path = out_file + ".count";
+  std::FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) return;
+  std::fprintf(f, "%s\t%llu\n", label.c_str(), (unsigned long long)n_tested);
+  std::fclose(f);
+  std::cerr << "[INFO] Count written to " << path << "\n";
 }
 
 // Text of the emitted rows (src/kgwas.cpp:239-259): default ostream float
@@ -436,29 +446,22 @@ static void run_rows(const Config& cfg) {  // src/kgwas.cpp:343-522
   kgio::Timer tall;
   Gpu g;
   g.start(cfg);
-  const auto all_ids = kgio::load_lines(cfg.samples_file);
-  const auto pheno = kgio::load_pheno(cfg.pheno_file);
-  vector<int> idxs;
-  vector<double> y;
-  for (int i = 0; i < (int)all_ids.size(); ++i) {
-    auto it = pheno.find(all_ids[i]);
-    if (it != pheno.end()) {
-      idxs.push_back(i);
-      y.push_back(it->second);
-    }
-  }
+  // ROWS mode words its input errors differently from COLS mode
+  // (src/kgwas.cpp:349-381): no check for an empty sample list, and U.bin is
+  // only checked for its row count.
+  const kgio::Overlap ov = kgio::match_phenotypes(kgio::read_sample_ids(cfg.samples_file), cfg.pheno_file);
+  const vector<int>& idxs = ov.idxs;
+  const vector<double>& y = ov.y;
   const int n = (int)idxs.size();
   if (n == 0) die("No overlapping genomes in phenotype.");
-  std::ifstream uin(cfg.U_file, std::ios::binary);
-  if (!uin) die("Cannot open " + cfg.U_file);
-  int n_u = 0, r = 0;
-  uin.read((char*)&n_u, sizeof(int));
-  uin.read((char*)&r, sizeof(int));
-  if (n_u != n)
-    die("U.bin row count (" + std::to_string(n_u) + ") does not match phenotype size (" + std::to_string(n) + ")");
-  if (r < 0) die("Cannot open " + cfg.U_file);
-  vector<double> U((size_t)n * r, 0.0);
-  uin.read((char*)U.data(), (std::streamsize)(sizeof(double) * (size_t)n * r));
+  const kgio::UbinFile uf = kgio::read_ubin_file(cfg.U_file);
+  if (uf.status == kgio::UbinFile::kNoFile) die("Cannot open " + cfg.U_file);
+  if (uf.n != n)
+    die("U.bin row count (" + std::to_string(uf.n) + ") does not match phenotype size (" + std::to_string(n) + ")");
+  if (uf.k < 0) die("Cannot open " + cfg.U_file);
+  const int r = uf.k;
+  vector<double> U((size_t)n * r, 0.0);  // a short body leaves zeros
+  std::copy(uf.U.begin(), uf.U.begin() + std::min(uf.U.size(), U.size()), U.begin());
   std::cerr << "[INFO] CORR_THRESHOLD=" << cfg.corr_threshold << "\n";
 
   kgio::RowsReader rr(cfg.input_path, cfg.LOAD_THREADS);

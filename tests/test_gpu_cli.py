@@ -75,19 +75,27 @@ def test_cli_matches_reference_cfg1(built):
             _check_outputs(out, "cfg1", mode, v, ds.kmers, band)
 
 
-def test_kbits_sidecar_reuse(built):
+@pytest.mark.parametrize("name", ["small", "edge"])
+def test_kbits_sidecar_reuse(built, name):
     """KGWAS_KBITS=1: the first run writes the packed rows next to the batch,
-    the second reads them back (no column files needed) with identical output."""
+    later runs read them back instead of the column files.  Every run, the
+    one that writes the sidecar and those that read it, must give the
+    reference's own files for the fixture (src/kgwas.cpp:225-304)."""
     import glob
     import shutil
+    fx = H.load_fixture(name)
+    n = int(fx["idxs"].shape[0])
     work = tempfile.mkdtemp()
-    paths, _ = H.materialise("small", work)
-    outs = []
-    for i in range(2):
+    paths, _ = H.materialise(name, work)
+    variants = H.meta(name)["variants"]
+    for i, v in enumerate([variants[0]] + variants):
+        st = O.cols_stats(fx["packed"], n, fx["U"], fx["y"], _thr(v))
+        band = H.band_kmers(st, _thr(v), _log10(v))
         out = os.path.join(work, f"run{i}", "batch_000.tsv")
         os.makedirs(os.path.dirname(out))
-        r = H.run_cli([paths["samples"], paths["pheno"], paths["batch"], paths["ubin"], out, "2"],
-                      {"KGWAS_KBITS": "1"})
+        env = dict(v.get("env", {}), KGWAS_KBITS="1")
+        r = H.run_cli([paths["samples"], paths["pheno"], paths["batch"], paths["ubin"], out, *v["args"],
+                       "--mode", "cols"], env)
         assert r.returncode == 0, r.stderr[-2000:]
         if i == 0:
             assert len(glob.glob(os.path.join(paths["batch"], "*.kbits"))) == 1
@@ -95,12 +103,12 @@ def test_kbits_sidecar_reuse(built):
             # length, so N is still inferred), which would change the output
             # if the columns were read again
             for f in glob.glob(os.path.join(paths["batch"], "bits", "col_*.txt")):
+                length = len(open(f).readline().rstrip("\n"))
                 with open(f, "w") as fh:
-                    fh.write("0" * 3000 + "\n")
+                    fh.write("0" * length + "\n")
         else:
             assert "packed rows from" in r.stderr
-        outs.append((open(out).read(), open(out + ".count").read()))
-    assert outs[0] == outs[1]
+        _check_outputs(out, name, "cols", v, fx["kmers"], band)
     shutil.rmtree(work)
 
 

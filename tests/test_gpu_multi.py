@@ -41,20 +41,29 @@ def oracle_pheno(packed_all, n_all, U, y, keep, thr):
     return O.cols_stats(synth.select_samples(packed_all, n_all, keep), keep.size, U, y, thr)
 
 
-@pytest.mark.parametrize("kernel", ["stationary", "streamed"])
+KERNEL_NAME = {"mpb": "image resident (mpb)", "mpb2": "SM pair, cta_group::2 (mpb2)", "mp": "image streamed (mp)"}
+
+
+@pytest.mark.parametrize("kernel", ["mpb", "mpb2", "mp"])
 @pytest.mark.parametrize("case", [(1000, 6000, 5, (16,), 16), (2000, 3000, 9, (20, 4), 32),
-                                  (300, 2500, 7, (3, 6), 16)], ids=["n1000_r16", "n2000_r20", "n300_r3"])
+                                  (300, 2500, 7, (3, 6), 16), (1000, 7001, 5, (20, 18), 16)],
+                         ids=["n1000_r16", "n2000_r20", "n300_r3", "n1000_r20"])
 def test_multi_matches_oracle(built, case, kernel, monkeypatch):
-    """Both many-phenotype kernels: the B image resident in shared memory
-    (kernel_mpb.cu) and streamed from L2 per 128 samples (kernel_mp.cu)."""
-    if kernel == "streamed":
-        monkeypatch.setenv("KG_MP_STREAMED", "1")
+    """Every many-phenotype kernel: one phenotype group's limb image resident
+    in shared memory (kernel_mpb.cu), two phenotypes per M = 256 MMA on a
+    pair of SMs (kernel_mpb2.cu, where one phenotype fills a group), and the
+    image streamed from L2 per 128 samples (kernel_mp.cu)."""
+    monkeypatch.setenv("KG_MP_KERNEL", kernel)
     n_all, m, npheno, rl, wpk = case
     packed, phenos = make_batch(n_all, m, npheno, rl, seed=n_all + m, wpk=wpk)
     shards = np.array([0, 7, m // 3, m // 3 + 1, m - 5], dtype=np.uint64)
     with api.Kgwas(corr_threshold=0.0, log10_thresh=0.0) as g:     # every tested k-mer is a row
         g.set_phenotypes(phenos, n_all)
         tested, hits = g.run_multi_host(packed, shards)
+        used = g.multi_shape()["kernel"]
+    if kernel == "mpb2" and used != KERNEL_NAME["mpb2"]:
+        pytest.skip("these phenotypes share an MMA group on one SM (the pair kernel needs NP >= 48 and PPG = 1)")
+    assert used == KERNEL_NAME[kernel]
     bounds = list(shards.astype(int)) + [m]
     for p, (U, y, keep) in enumerate(phenos):
         o = oracle_pheno(packed[:, :synth.words_per_kmer(n_all)], n_all, U, y, keep, 0.0)
@@ -85,11 +94,13 @@ def test_multi_matches_single_phenotype_api(built):
         assert np.allclose(h["chisq"], r.hits["chisq"], rtol=1e-12, atol=0)
 
 
-def test_multi_graph_replay(built):
-    """Repeated device launches with the same rows replay a captured CUDA graph."""
+@pytest.mark.parametrize("r", [16, 20])
+def test_multi_graph_replay(built, r):
+    """Repeated device launches with the same rows replay a captured CUDA
+    graph (r = 20: the SM-pair kernel's cluster launch inside the graph)."""
     import torch
     n_all, m = 1000, 30000
-    packed, phenos = make_batch(n_all, m, 4, (16,), seed=5)
+    packed, phenos = make_batch(n_all, m, 4, (r,), seed=5)
     dx = torch.from_numpy(packed.view(np.int64)).cuda()
     st = torch.cuda.current_stream().cuda_stream
     outs = []
@@ -119,25 +130,47 @@ def test_multi_streamed_chunks_match_single_chunk(built, monkeypatch):
 
 
 def test_multi_kernels_bit_identical(built, monkeypatch):
-    """The B-stationary and streamed-B kernels give the same counts and the
-    same rows bit for bit (same limb image, same exact integer sums), also
-    with several L2 blocks per launch and a partial last block."""
+    """The three many-phenotype kernels give the same counts and the same
+    rows bit for bit (same limb image, same exact integer sums), also with
+    several L2 blocks per launch and a partial last block and pair-tile."""
     n_all, m = 2000, 50000
-    packed, phenos = make_batch(n_all, m, 6, (20, 9), seed=23, wpk=32)
+    packed, phenos = make_batch(n_all, m, 7, (20, 9), seed=23, wpk=32)
     shards = np.array([0, 4096, 30001], dtype=np.uint64)
     out = {}
-    for kernel, bt in (("stationary", None), ("stationary", "2"), ("streamed", None)):
-        monkeypatch.delenv("KG_MP_STREAMED", raising=False)
+    for kernel, bt in (("mpb", None), ("mpb", "2"), ("mpb2", None), ("mpb2", "3"), ("mp", None)):
+        monkeypatch.setenv("KG_MP_KERNEL", kernel)
         monkeypatch.delenv("KG_MP_BT", raising=False)
-        if kernel == "streamed":
-            monkeypatch.setenv("KG_MP_STREAMED", "1")
         if bt:
             monkeypatch.setenv("KG_MP_BT", bt)
         with api.Kgwas(corr_threshold=0.0, log10_thresh=1.0) as g:
             g.set_phenotypes(phenos, n_all)
             out[(kernel, bt)] = g.run_multi_host(packed, shards)
-    t0, h0 = out[("streamed", None)]
-    for key in (("stationary", None), ("stationary", "2")):
+            assert g.multi_shape()["kernel"] == KERNEL_NAME[kernel]
+    t0, h0 = out[("mp", None)]
+    for key in (("mpb", None), ("mpb", "2"), ("mpb2", None), ("mpb2", "3")):
         t, h = out[key]
         assert np.array_equal(t, t0), key
         assert np.array_equal(h, h0), key
+
+
+def test_multi_autotuner_picks_a_measured_shape(built):
+    """Without a kernel request the autotuner times the candidate shapes and
+    keeps one; the result equals the streamed kernel's."""
+    import os
+    n_all, m = 2000, 60000
+    packed, phenos = make_batch(n_all, m, 4, (20,), seed=29, wpk=32)
+    assert "KG_MP_KERNEL" not in os.environ
+    with api.Kgwas(corr_threshold=0.0, log10_thresh=1.0) as g:
+        g.set_phenotypes(phenos, n_all)
+        t1, h1 = g.run_multi_host(packed)
+        shape = g.multi_shape()
+    assert shape["kernel"] in KERNEL_NAME.values() and shape["bt"] >= 1
+    os.environ["KG_MP_KERNEL"] = "mp"
+    try:
+        with api.Kgwas(corr_threshold=0.0, log10_thresh=1.0) as g:
+            g.set_phenotypes(phenos, n_all)
+            t2, h2 = g.run_multi_host(packed)
+    finally:
+        del os.environ["KG_MP_KERNEL"]
+    assert np.array_equal(t1, t2)
+    assert np.array_equal(h1, h2)

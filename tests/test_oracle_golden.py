@@ -18,7 +18,7 @@ import helpers as H
 from oracle import oracle as O
 
 ROWS_REL = 1.1e-5    # 6 printed significant digits: one unit in the last digit is <= 1e-5 relative
-COLS_REL = 2e-2      # reference COLS computes xxM/xyM in FP32 (measured <= 6.5e-3)
+COLS_REL = 1e-2      # reference COLS computes xxM/xyM in FP32 (measured <= 6.5e-3 on these fixtures)
 
 
 def _thr(variant):
