@@ -113,11 +113,11 @@ def reference_binary():
     return exe if os.access(exe, os.X_OK) else None
 
 
-def cpu_reference_run(n, m_sample, r, seed, threads, workdir):
+def cpu_reference_run(n, m_sample, r, seed, threads, workdir, S=None):
     """Run the reference kgwas (COLS mode) on an m_sample-k-mer batch; returns (tests, seconds)."""
     from supergwas_b200 import synth
     from oracle import oracle as O
-    ds = synth.simulate(n=n, m=m_sample, S=WORKLOAD["S"], r=r, n_causal=min(50, m_sample),
+    ds = synth.simulate(n=n, m=m_sample, S=S or WORKLOAD["S"], r=r, n_causal=min(50, m_sample),
                         missing=WORKLOAD["missing"], seed=seed, structure_kmers=min(50_000, m_sample))
     paths = synth.write_dataset(workdir, ds)
     out = os.path.join(workdir, "out", "batch_000.tsv")
@@ -540,69 +540,148 @@ def fp64_config2_leg(X, local, rank, steps, warmup, fp64_peak):
                      "peak_source": "measured (kg_probe_fp64_tflops: DFMA chains on every SM)"}}
 
 
-STREAMING = dict(n=5000, m=24_000_000, S=12, r=32, n_pheno=8, seed=47)
+STREAMING = dict(n=5000, S=12, r=32, n_pheno=8, seed=47, m_total=1_000_000_000, chunk_bytes=16_000_000_000,
+                 chunks=8, fp64_kmers=2_000_000, acc_kmers=20_000, cpu_kmers=200_000)
 
 
 def run_streaming(args):
-    """Streaming workload: rows live in pinned host memory and every step
-    streams them through kg_run_multi_host (chunked host-to-device copies on
-    a side stream overlapped with the fused kernel), 8 phenotypes."""
-    import ctypes
+    """Large streaming workload (n=5000 in 12 subpopulations, r=32+1, 8
+    phenotypes with their own missing masks, m=1e9 k-mers = 625 GB of packed
+    rows).  The rows live in pinned host memory in 16 GB chunks and stream
+    through kg_run_multi_host (chunked host-to-device copies overlapped with
+    the fused kernels).  625 GB does not fit host memory, so each chunk is
+    regenerated from its own seed while the previous one is tested: the
+    device generator writes chunk c+1 and copies it into the other pinned
+    buffer (device-to-host, the other direction of the link) while chunk c
+    streams in.  --steps chunks are timed (the per-chunk rate is steady; the
+    line extrapolates the whole 1e9).  Also: the plain FP64 form on a
+    device-resident sample of every phenotype, the split form's accuracy
+    against the FP64 oracle, and the reference kgwas on a slice."""
+    import threading
     import torch
     from supergwas_b200 import api, build, synth_gpu, synth
+    from oracle import oracle as O
     rank, world, local = rank_env()
     torch.cuda.set_device(local)
     build.build_all()
     W = dict(STREAMING)
-    if args.kmers:
-        W["m"] = args.kmers
-    n, m, r, npn = W["n"], W["m"], W["r"], W["n_pheno"]
+    n, S, r, npn, seed = W["n"], W["S"], W["r"], W["n_pheno"], W["seed"] + 1000 * rank
     wpk = synth.words_per_kmer(n)
-    nbytes = m * wpk * 8
+    row = wpk * 8
+    per = args.kmers or int(W["chunk_bytes"] // row)          # 25,000,000 rows = 16 GB at n=5000
+    nchunks = max(1, args.steps)
     t_gen = time.perf_counter()
-    hbuf = api.lib().kg_host_alloc(nbytes)
-    if not hbuf:
-        raise RuntimeError("kg_host_alloc failed")
-    ht = torch.frombuffer((ctypes.c_char * nbytes).from_address(hbuf), dtype=torch.int64).view(m, wpk)
-    step = 4_000_000
-    phenos = None
-    for s0 in range(0, m, step):
-        cnt = min(step, m - s0)
-        X = synth_gpu.gen_packed(n, cnt, W["S"], W["seed"] * 7919 + s0 // step)
-        if phenos is None:
-            phenos = synth_gpu.batched_phenotypes(X, n, npn, r, W["seed"], structure_kmers=min(cnt, 20_000))
-        ht[s0:s0 + cnt].copy_(X)
-        del X
+    dgen = torch.empty((per, wpk), dtype=torch.int64, device="cuda")
+    hbuf = [torch.empty((per, wpk), dtype=torch.int64, pin_memory=True) for _ in range(2)]
+    gs = torch.cuda.Stream()
+    gen_s = []
+
+    def produce(c, b):
+        t = time.perf_counter()
+        synth_gpu.synth_rows(dgen, n, S, seed, first=c * per, stream=gs)
+        with torch.cuda.stream(gs):
+            hbuf[b].copy_(dgen, non_blocking=True)
+        gs.synchronize()
+        gen_s.append(time.perf_counter() - t)
+
+    produce(0, 0)
+    phenos = synth_gpu.batched_phenotypes(dgen, n, npn, r, seed, structure_kmers=20_000)
     torch.cuda.synchronize()
     t_gen = time.perf_counter() - t_gen
+    h2d_peak = api.probe_h2d_gbs(local, 1 << 30, 8)
     g = api.Kgwas(device=local, precision="split", corr_threshold=0.0, log10_thresh=6.0)
     g.set_phenotypes(phenos, n)
-    for _ in range(args.warmup):
-        g.run_multi_host(np.ctypeslib.as_array((ctypes.c_uint64 * (m * wpk)).from_address(hbuf)).reshape(m, wpk))
-    view = np.ctypeslib.as_array((ctypes.c_uint64 * (m * wpk)).from_address(hbuf)).reshape(m, wpk)
+    view = [h.numpy().view(np.uint64) for h in hbuf]
+    warm = min(per, 2_000_000)
+    for _ in range(max(1, args.warmup)):
+        g.run_multi_host(view[0][:warm])
+    shape = g.multi_shape()
+    chunk_s, tests = [], 0.0
+    hits_total = 0
     with Clocks(local) as ck:
         t0 = time.perf_counter()
-        tests = 0.0
-        for _ in range(args.steps):
-            tested, hits = g.run_multi_host(view)
+        for c in range(nchunks):
+            th = None
+            if c + 1 < nchunks:
+                th = threading.Thread(target=produce, args=(c + 1, (c + 1) % 2))
+                th.start()
+            tc = time.perf_counter()
+            tested, hits = g.run_multi_host(view[c % 2])
+            chunk_s.append(time.perf_counter() - tc)
             tests += float(tested.sum())
+            hits_total += int(hits.shape[0])
+            if th is not None:
+                th.join()
         t = time.perf_counter() - t0
+    launches = g.last_launch_count()
     value = tests / t
-    line = {"metric": "k-mer tests/s (streaming from pinned host: 8 phenotypes, n=5000, r=32+1)",
-            "value": value, "unit": "k-mer tests/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "i8 limbs -> i32 TMEM, f64 epilogue", "data": "synthetic (seeded, generated on device)",
-            "config": {"workload": f"streaming: n={n}, {m} k-mers per step ({nbytes / 1e9:.1f} GB pinned host "
-                                   f"batch of the m=1e9 workload), r={r}+1, {npn} phenotypes, CORR_THRESHOLD=0",
+    kmers_per_s = nchunks * per / t
+    # accuracy of the split form on a sample of the last chunk, every phenotype, vs the FP64 oracle
+    m_acc = min(per, W["acc_kmers"])
+    Xh = view[(nchunks - 1) % 2][:m_acc].copy()
+    with api.Kgwas(device=local, precision="split", corr_threshold=0.0, log10_thresh=0.0) as ga:
+        ga.set_phenotypes(phenos, n)
+        _, ah = ga.run_multi_host(Xh)
+    acc = []
+    for p in range(npn):
+        U, y, keep = phenos[p]
+        o = O.cols_stats(synth.select_samples(Xh, n, keep), keep.size, U, y, 0.0)
+        h = ah[ah["pheno"] == p]
+        exp = np.nonzero(o["tested"])[0]
+        same = np.array_equal(h["kmer"].astype(np.int64), exp)
+        ml = np.abs(O.mlog10p(h["chisq"]) - o["mlog10p"][exp]) if same else np.array([np.inf])
+        T0, T1 = (o["chisq"][exp], h["chisq"]) if same else (np.ones(1), np.full(1, np.inf))
+        rel = np.abs(T1 - T0) / np.maximum(T0, 1e-300)
+        acc.append({"pheno": p, "n": int(keep.size), "tested_identical": bool(same),
+                    "mlog10p_abs_max": float(ml.max()), "chisq_rel_p99": float(np.percentile(rel, 99))})
+    # plain FP64 form, every phenotype, on a device-resident sample (the last chunk's rows)
+    m64 = min(per, W["fp64_kmers"])
+    dgen[:m64].copy_(hbuf[(nchunks - 1) % 2][:m64])
+    st = torch.cuda.Stream()
+    f_tests, f_t = 0.0, 0.0
+    for U, y, keep in phenos:
+        with api.Kgwas(device=local, precision="fp64", corr_threshold=0.0, log10_thresh=6.0) as f:
+            f.set_structure(U, y, keep, n)
+            tt, per_ms, _ = time_device(f, dgen[:m64], m64, wpk, 2, 1, st)
+        f_tests += tt
+        f_t += sum(per_ms) / len(per_ms) / 1e3
+    fp64_value = f_tests / f_t
+    # the reference kgwas (one phenotype per process, as the pipeline runs it) on a slice
+    cpu = None
+    if not args.no_cpu and reference_binary() and rank == 0:
+        threads = os.cpu_count() or 1
+        with tempfile.TemporaryDirectory() as d:
+            tested_ref, dt, _ = cpu_reference_run(n, W["cpu_kmers"], r, W["seed"], threads, d, S=S)
+        cpu = {"value": tested_ref / dt, "unit": "k-mer tests/s", "cores": threads, "kind": "reference",
+               "sample": f"reference kgwas --mode cols, one phenotype, n={n}, r={r}+1, {W['cpu_kmers']} k-mers, "
+                         "CORR_THRESHOLD=0, wall clock incl. its file load; a test is one (k-mer, phenotype), so "
+                         "the rate carries over to 8 phenotypes run as 8 processes"}
+    h2d_gbs = nchunks * per * row / sum(chunk_s) / 1e9
+    line = {"metric": "k-mer tests/s (streaming from pinned host: 8 phenotypes, n=5000, r=32+1, 16 GB chunks)",
+            "value": value, "unit": "k-mer tests/s", "n_gpus": world, "steps": nchunks, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t / nchunks, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "i8 limbs -> i32 TMEM, f64 epilogue",
+            "data": "synthetic (seeded Balding-Nichols, each chunk regenerated on the device from its seed)",
+            "config": {"workload": f"streaming: n={n} ({S} subpopulations), m=1e9 k-mers as {W['m_total'] // per} "
+                                   f"chunks of {per} ({per * row / 1e9:.1f} GB) in pinned host memory, r={r}+1, "
+                                   f"{npn} phenotypes (0-30% missing each), CORR_THRESHOLD=0; {nchunks} chunks timed",
                        "parallelism": f"weak: {world} GPU(s)"},
-            "e2e": {"value": value, "unit": "k-mer tests/s", "h2d_bytes_per_step": nbytes,
-                    "d2h_bytes_per_step": int(hits.shape[0]) * 40 + npn * 8},
-            "h2d_gbs": nbytes * args.steps / t / 1e9, "kmers_per_s": m * args.steps / t,
-            "gpu_launches": g.last_launch_count(), "clocks": ck.summary(), "gen_seconds": t_gen}
+            "tile_shape": shape,
+            "e2e": {"value": value, "unit": "k-mer tests/s", "h2d_bytes_per_step": per * row,
+                    "d2h_bytes_per_step": hits_total * 40 // nchunks + npn * 8, "api": "kg_run_multi_host"},
+            "roofline": {"bound": "host link", "achieved": h2d_gbs, "peak": h2d_peak, "unit": "GB/s",
+                         "frac": h2d_gbs / h2d_peak if h2d_peak else None,
+                         "peak_source": "measured (kg_probe_h2d_gbs, 8 x 1 GiB pinned)", "traffic": None},
+            "kmers_per_s": kmers_per_s, "full_1e9_seconds_extrapolated": W["m_total"] / kmers_per_s,
+            "chunk_seconds": chunk_s, "regen_seconds": gen_s[1:],
+            "fp64_form": {"value": fp64_value, "unit": "k-mer tests/s",
+                          "sample": f"{m64} device-resident k-mers x {npn} phenotypes",
+                          "split_speedup": value / world / fp64_value},
+            "accuracy_vs_fp64_oracle": acc, "cpu_baseline": cpu,
+            "gpu_launches": launches, "clocks": ck.summary(), "gen_seconds": t_gen}
     if rank == 0:
         print(json.dumps(line), flush=True)
     g.close()
-    api.lib().kg_host_free(hbuf)
 
 
 SORTED = dict(n=1000, m=50_000_000, S=8, r=16, n_causal=50, missing=0.05, seed=49, mean_run=5)
@@ -953,6 +1032,43 @@ def run_profile(args):
     g.close()
 
 
+def run_mma_rate(args):
+    """Back-to-back tcgen05.mma kind::i8 rates per SM (libkgwas_bench.so):
+    the ceiling of the association kernels' contractions.  One JSON line; the
+    rows give cycles per MMA of one issuing stream and int8 MACs per SM-cycle
+    against the 8192 of the hardware."""
+    import ctypes
+    import torch
+    from supergwas_b200 import build
+    rank, world, local = rank_env()
+    torch.cuda.set_device(local)
+    build.build_all()
+    L = ctypes.CDLL(build.BENCH_LIB)
+    L.kg_bench_mma_rate.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_ulonglong)]
+    names = {0: "one CTA per SM", 1: "two CTAs per SM", 2: "CTA pair, cta_group::2 (M=256)",
+             3: "one CTA per SM, 4 warps storing to TMEM", 4: "one CTA per SM, 4 warps loading from TMEM"}
+    table = [(0, 32, 1), (0, 64, 1), (0, 80, 1), (0, 128, 1), (0, 160, 1), (0, 256, 1), (0, 32, 2), (0, 64, 2),
+             (0, 64, 4), (1, 64, 1), (2, 64, 1), (2, 128, 1), (2, 160, 1), (2, 256, 1), (3, 64, 1), (3, 128, 1),
+             (4, 64, 1), (4, 128, 1)]
+    rows = []
+    for kind, N, iss in table:
+        cyc, side, err = ctypes.c_double(), ctypes.c_double(), ctypes.c_ulonglong()
+        rc = L.kg_bench_mma_rate(kind, N, iss, ctypes.byref(cyc), ctypes.byref(side), ctypes.byref(err))
+        if rc != 0:
+            rows.append({"setup": names[kind], "N": N, "issuers": iss, "rc": rc})
+            continue
+        M = 256 if kind == 2 else 128
+        streams = iss * (2 if kind == 1 else 1)
+        per_sm_macs = 128.0 * N * 32 * streams / cyc.value  # each SM computes 128 rows per instruction
+        rows.append({"setup": names[kind], "M": M, "N": N, "issuers": iss, "cycles_per_mma": cyc.value,
+                     "int8_macs_per_sm_cycle": per_sm_macs, "frac_of_8192": per_sm_macs / 8192.0,
+                     "side_cycles_per_tmem_op": side.value if kind >= 3 else None, "wait_errors": err.value})
+    if rank == 0:
+        print(json.dumps({"metric": "tcgen05.mma kind::i8 rate per SM (4096 back-to-back MMAs, K=32)",
+                          "unit": "int8 MACs per SM-cycle", "rows": rows}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -969,12 +1085,13 @@ def main():
     ap.add_argument("--no-legs", action="store_true",
                     help="default workload only: skip the FP64 n=1000/r=10 and the batched 64-phenotype legs")
     ap.add_argument("--workload", default="precision",
-                    choices=["precision", "batched", "streaming", "pairs", "sorted", "files", "profile"],
+                    choices=["precision", "batched", "streaming", "pairs", "sorted", "files", "profile", "mma-rate"],
                     help="precision: the default single-phenotype workload; batched: 64 phenotypes; "
                          "streaming: 8 phenotypes at n=5000 from pinned host memory; pairs: the 2-D pair test; "
                          "sorted: end to end on a batch with runs of equal rows; "
                          "files: the kgwas program against the reference's on the same files; "
-                         "profile: a few launches of one kernel for ncu (--kernel, --launches, --n, --r, --pheno)")
+                         "profile: a few launches of one kernel for ncu (--kernel, --launches, --n, --r, --pheno); "
+                         "mma-rate: tcgen05 MMA rates per SM")
     ap.add_argument("--kernel", default="ts", choices=["ts", "ss", "fp64", "multi", "pairs"])
     ap.add_argument("--launches", type=int, default=3)
     ap.add_argument("--n", type=int, default=1000, help="samples (profile workload)")
@@ -997,6 +1114,8 @@ def main():
         run_files(args)
     elif args.workload == "profile":
         run_profile(args)
+    elif args.workload == "mma-rate":
+        run_mma_rate(args)
     else:
         run_ours(args)
 

@@ -261,8 +261,9 @@ const char* kg_last_kernel(const kg_ctx* ctx);
 uint64_t kg_last_unique_rows(const kg_ctx* ctx);
 
 /* Bounded device-side waits.  Every wait between the roles of the
- * association kernels' pipelines (row loads, tensor-memory slots,
- * accumulators) gives up after wait_ns nanoseconds: the kernel then stops,
+ * tensor-memory kernels' pipelines (row loads, tensor-memory slots,
+ * accumulators, limb images; the single-phenotype, many-phenotype and pair
+ * kernels) gives up after wait_ns nanoseconds: the kernel then stops,
  * waits for its own copies and MMAs in flight, frees its tensor memory and
  * returns, and the call reports KG_ERR_TIMEOUT while the context stays
  * usable.  0 restores the default of 2 s.  The reference has no device waits;

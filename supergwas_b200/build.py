@@ -21,6 +21,8 @@ CSRC = os.path.join(PKG, "csrc")
 LIB_DIR = os.path.join(PKG, "lib")
 BIN_DIR = os.path.join(PKG, "bin")
 LIB = os.path.join(LIB_DIR, "libkgwas_cuda.so")
+BENCH_LIB = os.path.join(LIB_DIR, "libkgwas_bench.so")  # bench-side device code (generator, MMA-rate kernels)
+BENCH_SOURCES = ["bench_synth.cu", "bench_mma_rate.cu"]
 CLI = os.path.join(BIN_DIR, "kgwas")
 CLI2 = os.path.join(BIN_DIR, "kgwas_2d")
 MERGE = os.path.join(BIN_DIR, "kgwas_index_merge")
@@ -100,8 +102,21 @@ def build_cli(force=False, verbose=False, target=None, sources=None) -> str:
     return target
 
 
+def build_bench(force=False, verbose=False) -> str:
+    """Bench-side device code, not the association library: the seeded
+    generator of synthetic batches and the tensor-core rate kernels."""
+    srcs = [os.path.join(CSRC, f) for f in BENCH_SOURCES]
+    if not force and _newer(BENCH_LIB, srcs + [os.path.join(CSRC, "device.cuh"), os.path.abspath(__file__)]):
+        return BENCH_LIB
+    os.makedirs(LIB_DIR, exist_ok=True)
+    run([nvcc(), *ARCH, "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared", "-o", BENCH_LIB, *srcs],
+        verbose)
+    return BENCH_LIB
+
+
 def build_all(force=False, verbose=False):
     build_lib(force, verbose)
+    build_bench(force, verbose)
     build_cli(force, verbose)
     build_cli(force, verbose, CLI2, CLI2_SOURCES)
     build_cli(force, verbose, MERGE, MERGE_SOURCES)

@@ -1,0 +1,299 @@
+// bench_mma_rate.cu -- measurement kernels behind the rate figures of the
+// association kernels (libkgwas_bench.so; run by `bench.py --workload
+// mma-rate`, not part of the association library).
+//
+// kg_bench_mma_rate times back-to-back tcgen05.mma kind::i8 instructions
+// (K = 32, accumulating) per SM:
+//   kind 0: one CTA per SM, `issuers` warps (on different SM sub-partitions)
+//           each issuing into its own accumulator;
+//   kind 1: two CTAs per SM (256 tensor-memory columns each), one issuer each;
+//   kind 2: a cluster of two CTAs issuing M = 256 MMAs (cta_group::2), B split
+//           over the pair, accumulators in both SMs' tensor memory;
+//   kind 3: kind 0 with one issuer while four other warps write tensor memory
+//           with tcgen05.st.32x32b.x32 (the A-operand stores of the unpack);
+//   kind 4: kind 0 with one issuer while four other warps read tensor memory
+//           with tcgen05.ld.32x32b.x16 (the accumulator loads of the epilogue).
+// A comes from tensor memory (M = 128 rows, 32 bytes of K per MMA), B from
+// shared memory.  Every wait is bounded (2 s); no TMA.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "device.cuh"
+
+using namespace kg;
+
+namespace {
+
+constexpr int kIters = 4096;
+
+__device__ __forceinline__ uint32_t sm_id() {
+  uint32_t s;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(s));
+  return s;
+}
+
+// out per CTA: [0] cycles of the MMA stream(s) (sum over issuers), [1]
+// tensor-memory transfers done by the side warps, [2] their cycles, [3] error bits
+template <int N, int ISS, int COLS, int SIDE>
+__global__ void __launch_bounds__(256, 512 / COLS) mma_single(unsigned long long* out, unsigned long long* errs) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t* g = smem_raw + (base - raw);
+  const uint32_t sB = base, bars = base + 8 * 32 * N;  // B: 8 K-steps of 32 x N bytes
+  __shared__ uint32_t s_tmem;
+  __shared__ unsigned long long s_mma[4];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int i = tid; i < 8 * 32 * N / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(g)[i] = 0x01010101u * (i & 3);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int w = 0; w < ISS; ++w) mbar_init(bars + 8 * w, 1);
+    mbar_fence_init();
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  unsigned long long* err = errs + (size_t)blockIdx.x * 4;
+  if (warp < ISS) {
+    const bool leader = elect_one();
+    constexpr uint32_t IDESC = idesc_i8(128, N);
+    const uint64_t bdesc0 = sdesc_noswz(sB, N * 16, 128);
+    constexpr uint32_t BSTEP = (2 * N * 16) >> 4;
+    const uint32_t d = tmem + warp * N;
+    const uint32_t a = tmem + ISS * N;  // 32 columns of A after the accumulators
+    __syncwarp();
+    const unsigned long long t0 = clock64();
+    if (leader) {
+      for (int it = 0; it < kIters; ++it) {
+        const int st = it & 7;
+        tc_mma_i8_ts(d, a + (st & 3) * 8, bdesc0 + st * BSTEP, IDESC, it ? 1u : 0u);
+      }
+      tc_commit(bars + 8 * warp);
+      mbar_wait(bars + 8 * warp, 0, err, 1);
+    }
+    __syncwarp();
+    if (leader) s_mma[warp] = clock64() - t0;
+  } else if (SIDE && warp >= 4) {
+    // side traffic on lane quarter (warp & 3), columns 256..287
+    const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + 256;
+    const unsigned long long t0 = clock64();
+    unsigned long long n = 0;
+    if (SIDE == 1) {
+      uint32_t o[32];
+#pragma unroll
+      for (int k = 0; k < 32; ++k) o[k] = (uint32_t)k * 0x01010101u;
+      for (int it = 0; it < kIters / 2; ++it, ++n) {
+        tc_st32(taddr, o);
+        tc_wait_st();
+      }
+    } else {
+      uint32_t acc = 0;
+      for (int it = 0; it < kIters; ++it, ++n) {
+        uint32_t r[16];
+        tc_ld16(taddr, r);
+        tc_wait_ld();
+        acc += r[0] ^ r[15];
+      }
+      if (acc == 0x12345678u) err[3] = acc;  // keeps the loads
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(out + (size_t)blockIdx.x * 4 + 1, n);
+      atomicAdd(out + (size_t)blockIdx.x * 4 + 2, clock64() - t0);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (tid == 0) {
+    unsigned long long s = 0;
+    for (int w = 0; w < ISS; ++w) s += s_mma[w];
+    out[(size_t)blockIdx.x * 4] = s;
+    out[(size_t)blockIdx.x * 4 + 3] = err[2] | ((unsigned long long)sm_id() << 32);
+  }
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(COLS) : "memory");
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+template <int N>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(128, 1)
+    mma_pair(unsigned long long* out, unsigned long long* errs) {
+  constexpr int NH = N / 2;  // B columns held by each CTA of the pair
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t* g = smem_raw + (base - raw);
+  const uint32_t sB = base, bar = base + 8 * 32 * NH;
+  __shared__ uint32_t s_tmem;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t rank = cluster_rank();
+  for (int i = tid; i < 8 * 32 * NH / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(g)[i] = 0x01010101u * (i & 3);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&s_tmem))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  unsigned long long* err = errs + (size_t)blockIdx.x * 4;
+  unsigned long long t0 = clock64();
+  if (rank == 0 && warp == 0) {
+    const bool leader = elect_one();
+    constexpr uint32_t IDESC = idesc_i8(256, N);
+    const uint64_t bdesc0 = sdesc_noswz(sB, NH * 16, 128);
+    constexpr uint32_t BSTEP = (2 * NH * 16) >> 4;
+    __syncwarp();
+    t0 = clock64();
+    if (leader) {
+      for (int it = 0; it < kIters; ++it) {
+        const int st = it & 7;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::i8 [%0], [%1], %2, %3, {%5, %5, %5, %5, %5, %5, %5, %5}, p;\n\t}" ::"r"(
+                tmem),
+            "r"(tmem + 256 + (st & 3) * 8), "l"(bdesc0 + st * BSTEP), "r"(IDESC), "r"(it ? 1u : 0u), "r"(0u)
+            : "memory");
+      }
+      asm volatile(
+          "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+              bar),
+          "h"((unsigned short)3)
+          : "memory");
+    }
+    __syncwarp();
+  }
+  if (tid == 0) mbar_wait(bar, 0, err, 1);
+  if (tid == 0) {
+    out[(size_t)blockIdx.x * 4] = rank == 0 ? clock64() - t0 : 0ull;  // the leader's stream
+    out[(size_t)blockIdx.x * 4 + 3] = err[2];
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();
+  tc_fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+}
+
+struct Result {
+  double cycles_per_mma = 0, side_cycles_per_op = 0;
+  unsigned long long err = 0;
+  int ok = 0;
+};
+
+template <class K>
+int launch_and_read(K kernel, int grid, int threads, int smem, int per_cta_streams, int side, Result& r) {
+  unsigned long long *d = nullptr, *e = nullptr;
+  if (cudaMalloc(&d, (size_t)grid * 4 * 8) != cudaSuccess) return 3;
+  if (cudaMalloc(&e, (size_t)grid * 4 * 8) != cudaSuccess) {
+    cudaFree(d);
+    return 3;
+  }
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  int rc = 0;
+  for (int rep = 0; rep < 3 && rc == 0; ++rep) {
+    cudaMemset(d, 0, (size_t)grid * 4 * 8);
+    cudaMemset(e, 0, (size_t)grid * 4 * 8);
+    kernel<<<grid, threads, smem>>>(d, e);
+    if (cudaDeviceSynchronize() != cudaSuccess) rc = 2;
+  }
+  if (rc == 0) {
+    std::vector<unsigned long long> h((size_t)grid * 4);
+    cudaMemcpy(h.data(), d, h.size() * 8, cudaMemcpyDeviceToHost);
+    double mma = 0, side_ops = 0, side_cyc = 0;
+    int ctas = 0;
+    for (int b = 0; b < grid; ++b) {
+      if (h[4 * b] == 0) continue;  // pair kernels: the peer issues nothing
+      mma += (double)h[4 * b];
+      side_ops += (double)h[4 * b + 1];
+      side_cyc += (double)h[4 * b + 2];
+      r.err |= h[4 * b + 3] & 0xffffffffull;
+      ++ctas;
+    }
+    r.cycles_per_mma = ctas ? mma / ((double)ctas * per_cta_streams * kIters) : 0.0;
+    r.side_cycles_per_op = side_ops > 0 ? side_cyc / side_ops : 0.0;
+    r.ok = ctas > 0 && r.err == 0;
+    (void)side;
+  }
+  cudaFree(d);
+  cudaFree(e);
+  return rc;
+}
+
+template <int N>
+int run_kind(int kind, int issuers, int sms, Result& r) {
+  switch (kind) {
+    case 0:
+      if (issuers == 1) return launch_and_read(mma_single<N, 1, 512, 0>, sms, 256, 150 * 1024, 1, 0, r);
+      if (issuers == 2 && 2 * N + 32 <= 512) return launch_and_read(mma_single<N, 2, 512, 0>, sms, 256, 150 * 1024, 2, 0, r);
+      if (issuers == 4 && 4 * N + 32 <= 512) return launch_and_read(mma_single<N, 4, 512, 0>, sms, 256, 150 * 1024, 4, 0, r);
+      return 1;
+    case 1:
+      if (N > 224) return 1;
+      return launch_and_read(mma_single<N, 1, 256, 0>, 2 * sms, 256, 100 * 1024, 1, 0, r);
+    case 2:
+      if (N % 32) return 1;
+      return launch_and_read(mma_pair<N>, sms & ~1, 128, 150 * 1024, 1, 0, r);
+    case 3:
+      if (N + 32 > 256) return 1;  // the side warps use columns 256..287
+      return launch_and_read(mma_single<N, 1, 512, 1>, sms, 256, 150 * 1024, 1, 1, r);
+    case 4:
+      if (N + 32 > 256) return 1;
+      return launch_and_read(mma_single<N, 1, 512, 2>, sms, 256, 150 * 1024, 1, 2, r);
+    default: return 1;
+  }
+}
+
+}  // namespace
+
+// Average cycles per MMA of one issuing stream (kinds 0, 1, 3, 4) or per
+// pair MMA (kind 2), and for kinds 3 and 4 the side warps' cycles per
+// tcgen05.st / tcgen05.ld.  Returns 0 on success, 1 for an unsupported
+// (kind, N, issuers), 2 for a CUDA error, 3 when out of memory; *err gets the
+// error bits of the bounded waits (0 when none gave up).
+extern "C" int kg_bench_mma_rate(int kind, int n_cols, int issuers, double* cycles_per_mma,
+                                 double* side_cycles_per_op, unsigned long long* err) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  Result r;
+  int rc = 1;
+  switch (n_cols) {
+    case 32: rc = run_kind<32>(kind, issuers, sms, r); break;
+    case 64: rc = run_kind<64>(kind, issuers, sms, r); break;
+    case 80: rc = kind == 2 ? 1 : run_kind<80>(kind, issuers, sms, r); break;
+    case 128: rc = run_kind<128>(kind, issuers, sms, r); break;
+    case 160: rc = run_kind<160>(kind, issuers, sms, r); break;
+    case 256: rc = kind == 1 ? 1 : run_kind<256>(kind, issuers, sms, r); break;
+    default: rc = 1;
+  }
+  if (cycles_per_mma) *cycles_per_mma = r.cycles_per_mma;
+  if (side_cycles_per_op) *side_cycles_per_op = r.side_cycles_per_op;
+  if (err) *err = r.err;
+  return rc;
+}

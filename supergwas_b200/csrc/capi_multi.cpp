@@ -114,6 +114,7 @@ kg::DevOutMP dev_out(kg_ctx* ctx, unsigned long long offset) {
   O.n_pheno = M.np;
   O.kmer_offset = offset;
   O.weight = ctx->cur_weight;
+  O.wait_ns = ctx->wait_ns;
   return O;
 }
 

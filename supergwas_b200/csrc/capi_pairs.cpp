@@ -175,7 +175,7 @@ int kg_pairs_run_host(kg_ctx* ctx, const uint64_t* xbits, uint64_t n_kmers, uint
   if ((rc = ensure_pair_cand(ctx, std::max<unsigned long long>(ctx->cand_cap, 1ull << 20)))) return rc;
   unsigned long long cnt[4] = {0, 0, 0, 0};
   for (int attempt = 0; attempt < 8; ++attempt) {
-    kg::DevOutPairs O{ctx->dCounters, ctx->dPairs, ctx->pair_cap, ctx->dCand, ctx->cand_cap};
+    kg::DevOutPairs O{ctx->dCounters, ctx->dPairs, ctx->pair_cap, ctx->dCand, ctx->cand_cap, ctx->wait_ns};
     KG_CUDA(cudaMemsetAsync(ctx->dCounters, 0, 4 * sizeof(unsigned long long), st), "memset");
     kg::LaunchPairs L{ctx->dPX, (int)wd, ctx->limbs.Kpad, ctx->prep.drop0 && ctx->P.k > 0, S, ctx->dBts, &ctx->P,
                       &ctx->LM, &O, ctx->num_sms};

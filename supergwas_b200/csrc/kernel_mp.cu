@@ -113,6 +113,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
+  const unsigned long long lim = wait_limit(O.wait_ns);
   const unsigned long long ntiles = (m + MP_TM - 1) / MP_TM;
 
   if (warp == MP_WARP_XP) {
@@ -123,7 +124,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
       uint32_t it = 0;
       for (unsigned long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
         const uint32_t xs = it % xs_slots, u = it / xs_slots;
-        if (u > 0 && !wait_or_abort(x_empty + 8 * xs, (u - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_FULL)) break;
+        if (u > 0 && !wait_or_abort(x_empty + 8 * xs, (u - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_FULL, lim)) break;
         mbar_arrive_expect_tx(x_full + 8 * xs, xslot);
         for (int bx = 0; bx < nbox; ++bx)
           tma_load_2d(sx + xs * xslot + bx * MP_BOXB, &tmap, bx * 128, (int)(tile * MP_TM), x_full + 8 * xs);
@@ -143,7 +144,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
         for (int gi = 0; gi < G && ok; ++gi)
           for (int kc = 0; kc < nchunk; ++kc, ++h) {
             const uint32_t s = h % nb, u = h / nb;
-            if (u > 0 && !wait_or_abort(b_empty + 8 * s, (u - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_FULL)) {
+            if (u > 0 && !wait_or_abort(b_empty + 8 * s, (u - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_FULL, lim)) {
               ok = false;
               break;
             }
@@ -162,15 +163,15 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
       for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         for (int gi = 0; gi < G && ok; ++gi, ++w) {
           const uint32_t b = w % NA, v = w / NA;
-          if (v > 0 && !wait_or_abort(acc_empty + 8 * b, (v - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA)) {
+          if (v > 0 && !wait_or_abort(acc_empty + 8 * b, (v - 1) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA, lim)) {
             ok = false;
             break;
           }
           tc_fence_after();
           for (int kc = 0; kc < nchunk; ++kc, ++g, ++h) {
             const uint32_t t = g % AST, s = h % nb;
-            if (!wait_or_abort(a_full + 8 * t, (g / AST) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA) ||
-                !wait_or_abort(b_full + 8 * s, (h / nb) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA)) {
+            if (!wait_or_abort(a_full + 8 * t, (g / AST) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA, lim) ||
+                !wait_or_abort(b_full + 8 * s, (h / nb) & 1, s_abort, O.counters, ERR_TIMEOUT_MMA, lim)) {
               ok = false;
               break;
             }
@@ -201,7 +202,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
     for (unsigned long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
       const uint32_t xs = it % xs_slots;
       if (!__all_sync(0xffffffffu, wait_or_abort(x_full + 8 * xs, (it / xs_slots) & 1, s_abort, O.counters,
-                                           ERR_TIMEOUT_FULL)))
+                                           ERR_TIMEOUT_FULL, lim)))
         break;
       const uint32_t tb = sx + xs * xslot;
       for (int gi = 0; gi < G && ok; ++gi) {
@@ -209,7 +210,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
           if ((int)(g % MP_UG) != grp) continue;
           const uint32_t t = g % AST, u = g / AST;
           if (u > 0 && !__all_sync(0xffffffffu, wait_or_abort(a_empty + 8 * t, (u - 1) & 1, s_abort, O.counters,
-                                                         ERR_TIMEOUT_MMA))) {
+                                                         ERR_TIMEOUT_MMA, lim))) {
             ok = false;
             break;
           }
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(MP_THREADS, 1)
       const bool leader = lane == __ffs(match) - 1;
       for (int gi = 0; gi < G; ++gi, ++w) {
         const uint32_t b = w % NA, v = w / NA;
-        if (!__all_sync(0xffffffffu, wait_or_abort(acc_full + 8 * b, v & 1, s_abort, O.counters, ERR_TIMEOUT_MMA))) {
+        if (!__all_sync(0xffffffffu, wait_or_abort(acc_full + 8 * b, v & 1, s_abort, O.counters, ERR_TIMEOUT_MMA, lim))) {
           ok = false;
           break;
         }

@@ -153,6 +153,7 @@ __global__ void __launch_bounds__(mb_threads(NP * PPG), 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
+  const unsigned long long lim = wait_limit(O.wait_ns);
 
   if (warp == WXP) {
     // ---------------------------------------------------------- x producer
@@ -170,7 +171,7 @@ __global__ void __launch_bounds__(mb_threads(NP * PPG), 1)
             const unsigned long long tile = blockIdx.x + i * gridDim.x;
             for (int bx = 0; bx < nbox; ++bx, xr.next()) {
               if (xr.used &&
-                  !wait_or_abort(x_empty + 8 * xr.slot, xr.phase ^ 1u, s_abort, O.counters, ERR_TIMEOUT_FULL)) {
+                  !wait_or_abort(x_empty + 8 * xr.slot, xr.phase ^ 1u, s_abort, O.counters, ERR_TIMEOUT_FULL, lim)) {
                 ok = false;
                 break;
               }
@@ -192,7 +193,7 @@ __global__ void __launch_bounds__(mb_threads(NP * PPG), 1)
       for (unsigned long long i0 = 0; i0 < nt && ok; i0 += BT)
         for (int g = 0; g < G && ok; ++g, ++pi) {
           // the previous pass's MMAs have read the resident image
-          if (pi > 0 && !wait_or_abort(b_free, (pi - 1) & 1u, s_abort, O.counters, ERR_TIMEOUT_FULL)) {
+          if (pi > 0 && !wait_or_abort(b_free, (pi - 1) & 1u, s_abort, O.counters, ERR_TIMEOUT_FULL, lim)) {
             ok = false;
             break;
           }
@@ -216,14 +217,14 @@ __global__ void __launch_bounds__(mb_threads(NP * PPG), 1)
     for (unsigned long long i0 = 0; i0 < nt && ok; i0 += BT) {
       const unsigned long long i1 = i0 + BT < nt ? i0 + BT : nt;
       for (int g = 0; g < G && ok; ++g, ++pi) {
-        if (!__all_sync(0xffffffffu, wait_or_abort(b_full, pi & 1u, s_abort, O.counters, ERR_TIMEOUT_MMA))) {
+        if (!__all_sync(0xffffffffu, wait_or_abort(b_full, pi & 1u, s_abort, O.counters, ERR_TIMEOUT_MMA, lim))) {
           ok = false;
           break;
         }
         for (unsigned long long i = i0; i < i1 && ok; ++i, ++v) {
           const uint32_t b = v & 1u;
           if (v >= 2 && !__all_sync(0xffffffffu, wait_or_abort(acc_empty + 8 * b, ((v >> 1) - 1) & 1u, s_abort,
-                                                               O.counters, ERR_TIMEOUT_MMA))) {
+                                                               O.counters, ERR_TIMEOUT_MMA, lim))) {
             ok = false;
             break;
           }
@@ -231,7 +232,7 @@ __global__ void __launch_bounds__(mb_threads(NP * PPG), 1)
           uint64_t bd = bdesc0;
           for (int sp = 0; sp < nsp; ++sp, ar.next()) {
             if (!__all_sync(0xffffffffu,
-                            wait_or_abort(a_full + 8 * ar.slot, ar.phase, s_abort, O.counters, ERR_TIMEOUT_MMA))) {
+                            wait_or_abort(a_full + 8 * ar.slot, ar.phase, s_abort, O.counters, ERR_TIMEOUT_MMA, lim))) {
               ok = false;
               break;
             }
@@ -289,7 +290,7 @@ __global__ void __launch_bounds__(mb_threads(NP * PPG), 1)
           int kc = 0;
           for (int bx = 0; bx < nbox && ok; ++bx, xr.next()) {
             if (!__all_sync(0xffffffffu,
-                            wait_or_abort(x_full + 8 * xr.slot, xr.phase, s_abort, O.counters, ERR_TIMEOUT_FULL))) {
+                            wait_or_abort(x_full + 8 * xr.slot, xr.phase, s_abort, O.counters, ERR_TIMEOUT_FULL, lim))) {
               ok = false;
               break;
             }
@@ -303,7 +304,7 @@ __global__ void __launch_bounds__(mb_threads(NP * PPG), 1)
                 continue;
               }
               if (ar.used && !__all_sync(0xffffffffu, wait_or_abort(a_empty + 8 * ar.slot, ar.phase ^ 1u, s_abort,
-                                                                    O.counters, ERR_TIMEOUT_MMA))) {
+                                                                    O.counters, ERR_TIMEOUT_MMA, lim))) {
                 ok = false;
                 break;
               }
@@ -352,7 +353,7 @@ __global__ void __launch_bounds__(mb_threads(NP * PPG), 1)
         for (unsigned long long i = i0; i < i1; ++i, ++v) {
           if ((v & 1u) != (uint32_t)e) continue;
           if (!__all_sync(0xffffffffu,
-                          wait_or_abort(acc_full + 8 * e, jt & 1u, s_abort, O.counters, ERR_TIMEOUT_MMA))) {
+                          wait_or_abort(acc_full + 8 * e, jt & 1u, s_abort, O.counters, ERR_TIMEOUT_MMA, lim))) {
             ok = false;
             break;
           }

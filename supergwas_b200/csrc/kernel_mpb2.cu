@@ -35,6 +35,8 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
+
 #include "device.cuh"
 #include "kernels.hpp"
 
@@ -550,8 +552,23 @@ static cudaError_t launch_mpb2_t(const LaunchMpb& L, const CUtensorMap& tm, cuda
   const size_t smem = mpb2_smem_bytes(NP, L.kpad);
   cudaError_t e = cudaFuncSetAttribute(mpb2_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  // as many pairs as can be resident at once (a GPC with an odd number of
+  // free SMs leaves one SM without a partner), else a second wave of pairs
+  // would double the launch
+  static int resident = -1;
+  if (resident < 0) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(L.num_sms & ~1));
+    cfg.blockDim = dim3(M2_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    int clusters = 0;
+    resident = cudaOccupancyMaxActiveClusters(&clusters, (void*)mpb2_kernel<NP>, &cfg) == cudaSuccess && clusters > 0
+                   ? clusters
+                   : L.num_sms / 2;
+    cudaGetLastError();
+  }
   const unsigned long long npt = (L.m + 2 * M2_TM - 1) / (2 * M2_TM);
-  unsigned long long pairs = (unsigned long long)(L.num_sms / 2);
+  unsigned long long pairs = (unsigned long long)std::min(L.num_sms / 2, resident);
   if (pairs > npt) pairs = npt;
   if (pairs < 1) pairs = 1;
   const int nbox = (L.wpk * 8 + 127) / 128;

@@ -170,6 +170,7 @@ __global__ void __launch_bounds__(pr_threads(N), 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
+  const unsigned long long lim = wait_limit(O.wait_ns);
 
   if (warp == WPROD) {
     // ------------------------------------------------------------ producer
@@ -188,7 +189,7 @@ __global__ void __launch_bounds__(pr_threads(N), 1)
       for (unsigned long long u = blockIdx.x; u < S.n_units && ok; u += gridDim.x) {
         const PairUnit U = pr_unit(S, u);
         for (int bx = 0; bx < nbox; ++bx, xr.next()) {
-          if (xr.used && !wait_or_abort(x_empty + 8 * xr.slot, xr.phase ^ 1u, s_abort, O.counters, ERR_TIMEOUT_FULL)) {
+          if (xr.used && !wait_or_abort(x_empty + 8 * xr.slot, xr.phase ^ 1u, s_abort, O.counters, ERR_TIMEOUT_FULL, lim)) {
             ok = false;
             break;
           }
@@ -205,7 +206,7 @@ __global__ void __launch_bounds__(pr_threads(N), 1)
   } else if (warp == WMMA) {
     // ----------------------------------------------------------------- MMA
     const bool leader = elect_one();
-    bool ok = __all_sync(0xffffffffu, wait_or_abort(b_full, 0, s_abort, O.counters, ERR_TIMEOUT_FULL));
+    bool ok = __all_sync(0xffffffffu, wait_or_abort(b_full, 0, s_abort, O.counters, ERR_TIMEOUT_FULL, lim));
     const uint64_t bdesc0 = sdesc_noswz(sb, N * 16, 128);
     Ring<NSLOT> ar;
     uint32_t v = 0;  // tiles
@@ -214,7 +215,7 @@ __global__ void __launch_bounds__(pr_threads(N), 1)
       for (unsigned long long i = U.i0; i < U.i1 && ok; ++i, ++v) {
         const uint32_t b = v & 1u;
         if (v >= 2 && !__all_sync(0xffffffffu, wait_or_abort(acc_empty + 8 * b, ((v >> 1) - 1) & 1u, s_abort,
-                                                             O.counters, ERR_TIMEOUT_MMA))) {
+                                                             O.counters, ERR_TIMEOUT_MMA, lim))) {
           ok = false;
           break;
         }
@@ -222,7 +223,7 @@ __global__ void __launch_bounds__(pr_threads(N), 1)
         uint64_t bd = bdesc0;
         for (int sp = 0; sp < nsp; ++sp, ar.next()) {
           if (!__all_sync(0xffffffffu,
-                          wait_or_abort(a_full + 8 * ar.slot, ar.phase, s_abort, O.counters, ERR_TIMEOUT_MMA))) {
+                          wait_or_abort(a_full + 8 * ar.slot, ar.phase, s_abort, O.counters, ERR_TIMEOUT_MMA, lim))) {
             ok = false;
             break;
           }
@@ -277,7 +278,7 @@ __global__ void __launch_bounds__(pr_threads(N), 1)
         int kc = 0;
         for (int bx = 0; bx < nbox && ok; ++bx) {
           if (i == U.i0 && !__all_sync(0xffffffffu, wait_or_abort(x_full + 8 * bslot[bx], bphase[bx], s_abort,
-                                                                  O.counters, ERR_TIMEOUT_FULL))) {
+                                                                  O.counters, ERR_TIMEOUT_FULL, lim))) {
             ok = false;
             break;
           }
@@ -291,7 +292,7 @@ __global__ void __launch_bounds__(pr_threads(N), 1)
               continue;
             }
             if (ar.used && !__all_sync(0xffffffffu, wait_or_abort(a_empty + 8 * ar.slot, ar.phase ^ 1u, s_abort,
-                                                                  O.counters, ERR_TIMEOUT_MMA))) {
+                                                                  O.counters, ERR_TIMEOUT_MMA, lim))) {
               ok = false;
               break;
             }
@@ -347,7 +348,7 @@ __global__ void __launch_bounds__(pr_threads(N), 1)
       const PairUnit U = pr_unit(S, u);
       for (unsigned long long i = U.i0; i < U.i1; ++i, ++v) {
         if ((v & 1u) != (uint32_t)e) continue;
-        if (!__all_sync(0xffffffffu, wait_or_abort(acc_full + 8 * e, jt & 1u, s_abort, O.counters, ERR_TIMEOUT_MMA))) {
+        if (!__all_sync(0xffffffffu, wait_or_abort(acc_full + 8 * e, jt & 1u, s_abort, O.counters, ERR_TIMEOUT_MMA, lim))) {
           ok = false;
           break;
         }

@@ -106,6 +106,7 @@ struct DevOutPairs {
   unsigned long long hit_cap;
   unsigned long long* cand;      // i << 32 | j
   unsigned long long cand_cap;
+  unsigned long long wait_ns;    // pipeline wait limit in ns (0: WAIT_LIMIT_NS)
 };
 
 // Pair schedule: pairs (i, j), i < j, row_start <= i < row_end, j < n_kmers.

@@ -10,6 +10,8 @@ host from a 50,000-k-mer sample and the causal k-mers, exactly as in
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import torch
 
@@ -46,6 +48,31 @@ def gen_packed(n: int, m: int, S: int, seed: int, device: str = "cuda", chunk: i
         by = (bits.view(cm, W * 8, 8).to(torch.uint8) * weights).sum(-1, dtype=torch.int32).to(torch.uint8)
         out[s:e] = by.view(torch.int64).view(cm, W)
         del bits, by
+    return out
+
+
+_SYNTH = None
+
+
+def synth_rows(out: torch.Tensor, n: int, S: int, seed: int, first: int = 0, stream=None) -> torch.Tensor:
+    """Rows first .. first + out.shape[0] - 1 of a seeded batch from the CUDA
+    generator (lib/libkgwas_bench.so): the same Balding-Nichols model, each
+    row a function of (seed, row index) only, so a chunk of any batch can be
+    regenerated on its own.  ``out`` is an (m, words_per_kmer(n)) int64 tensor
+    on the device; the kernel runs on ``stream`` (default: the current one)."""
+    import ctypes
+    from . import build
+    global _SYNTH
+    if _SYNTH is None:
+        if not os.path.exists(build.BENCH_LIB):
+            raise RuntimeError(f"{build.BENCH_LIB} is not built; run `python -m supergwas_b200.build`")
+        _SYNTH = ctypes.CDLL(build.BENCH_LIB)
+        _SYNTH.kg_synth_rows.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p]
+    st = stream if stream is not None else torch.cuda.current_stream()
+    rc = _SYNTH.kg_synth_rows(out.data_ptr(), out.shape[0], n, out.shape[1], S, first, seed, st.cuda_stream)
+    if rc != 0:
+        raise RuntimeError(f"kg_synth_rows failed ({rc})")
     return out
 
 
