@@ -321,6 +321,11 @@ def run_ours(args):
     d2h = 3 * 8 + rr.hits.shape[0] * 32
     api.lib().kg_host_free(hbuf)
 
+    # the programs on files at a pipeline-sized batch (rank 0)
+    leg_files = None
+    if rank == 0 and args.files_kmers and not args.no_legs:
+        leg_files = files_cols_leg(X[:min(m, args.files_kmers)].cpu().numpy().view(np.uint64), n, U, y, keep, local)
+
     # measured peaks of the FP64 form and of the host link
     fp64_peak = api.probe_fp64_tflops(local)
     h2d_peak = api.probe_h2d_gbs(local, 1 << 30, 8)
@@ -385,6 +390,7 @@ def run_ours(args):
                           "fp64_tflops": 2.0 * m * (((n + 127) // 128) * 128) * 20 / t_fp64 / 1e12,
                           "fp64_frac": 2.0 * m * (((n + 127) // 128) * 128) * 20 / t_fp64 / 1e12 / fp64_peak},
             "fp64_config2": leg_fp64,
+            "files_cols": leg_files,
             "batched": leg_batched,
             "peaks": {"hbm_gbs": hbm, "hbm_source": peak_src, "bf16_tflops": bf16,
                       "fp64_tflops": fp64_peak, "fp64_source": "measured (kg_probe_fp64_tflops)",
@@ -779,6 +785,60 @@ def run_sorted(args):
 FILES = dict(n=1000, m=1_000_000, r=16, seed=50)
 
 
+def files_cols_leg(Xh, n, U, y, keep, local, seed=51):
+    """The drop-in comparison at a pipeline-sized batch: the rows Xh (all n
+    samples) written as one batch_*/ directory (n column files and a
+    kmers.txt.gz of random 31-mers) with samples.txt, phenotype.txt (the
+    phenotyped samples) and U.bin, then the reference's kgwas and bin/kgwas
+    in COLS mode on the same files (CORR_THRESHOLD=0, files in the page
+    cache, all host threads for both).  Wall clock of each process; bin/kgwas
+    runs twice and the second run counts (the first loads the CUDA libraries
+    from disk)."""
+    from supergwas_b200 import build, synth
+    from oracle import oracle as O
+    m = Xh.shape[0]
+    threads = os.cpu_count() or 1
+    env = {"CORR_THRESHOLD": "0", "LOAD_THREADS": str(threads), "BLAS_THREADS": str(threads),
+           "EMIT_THREADS": str(threads), "KGWAS_DEVICE": str(local)}
+    rng = np.random.default_rng(seed)
+    with tempfile.TemporaryDirectory() as d:
+        t_w = time.perf_counter()
+        samples = [f"S{i:05d}" for i in range(n)]
+        paths = dict(samples=os.path.join(d, "samples.txt"), pheno=os.path.join(d, "phenotype.txt"),
+                     ubin=os.path.join(d, "U.bin"), batch=os.path.join(d, "batch_000"))
+        synth.write_samples(paths["samples"], samples)
+        synth.write_pheno(paths["pheno"], [samples[i] for i in keep], y)
+        synth.write_ubin(paths["ubin"], U)
+        synth.write_batch(paths["batch"], Xh, n, synth.random_kmers_text(rng, m))
+        t_w = time.perf_counter() - t_w
+        args = [paths["samples"], paths["pheno"], paths["batch"], paths["ubin"]]
+
+        def run(tag, reference):
+            out = os.path.join(d, tag, "batch_000.tsv")
+            os.makedirs(os.path.dirname(out), exist_ok=True)
+            t0 = time.perf_counter()
+            if reference:
+                r = O.run_reference([*args, out, "6", "--mode", "cols"], env)
+            else:
+                r = subprocess.run([build.CLI, *args, out, "6", "--mode", "cols"], env=dict(os.environ, **env),
+                                   capture_output=True, text=True)
+            dt = time.perf_counter() - t0
+            if r.returncode != 0:
+                raise RuntimeError(f"{tag}: {r.stderr[-500:]}")
+            return open(out + ".count").read(), dt
+
+        run("warm", False)
+        c_ours, s_ours = run("ours", False)
+        c_ref, s_ref = run("ref", True) if reference_binary() else (None, None)
+    tested = int(c_ours.split("\t")[1])
+    return {"kmers": m, "ours_seconds": s_ours, "ours_tests_per_s": tested / s_ours,
+            "reference_seconds": s_ref, "reference_tests_per_s": tested / s_ref if s_ref else None,
+            "speedup": s_ref / s_ours if s_ref else None, "count_lines_identical": c_ours == c_ref,
+            "write_seconds": t_w, "threads": threads,
+            "workload": f"first {m} k-mers of the bench batch as pipeline files: {n} column files, kmers.txt.gz, "
+                        "COLS mode, CORR_THRESHOLD=0, files in the page cache"}
+
+
 def run_files(args):
     """End to end through the programs, as the pipeline calls them: the
     reference's kgwas and this package's bin/kgwas on the same files of one
@@ -1047,10 +1107,13 @@ def run_mma_rate(args):
     L.kg_bench_mma_rate.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_ulonglong)]
     names = {0: "one CTA per SM", 1: "two CTAs per SM", 2: "CTA pair, cta_group::2 (M=256)",
-             3: "one CTA per SM, 4 warps storing to TMEM", 4: "one CTA per SM, 4 warps loading from TMEM"}
+             3: "one CTA per SM, 4 warps storing to TMEM (one wait per store)",
+             4: "one CTA per SM, 4 warps loading from TMEM",
+             5: "one CTA per SM, 4 warps storing to TMEM (4 stores per wait)",
+             6: "no MMAs, 4 warps storing to TMEM (4 stores per wait)"}
     table = [(0, 32, 1), (0, 64, 1), (0, 80, 1), (0, 128, 1), (0, 160, 1), (0, 256, 1), (0, 32, 2), (0, 64, 2),
              (0, 64, 4), (1, 64, 1), (2, 64, 1), (2, 128, 1), (2, 160, 1), (2, 256, 1), (3, 64, 1), (3, 128, 1),
-             (4, 64, 1), (4, 128, 1)]
+             (4, 64, 1), (4, 128, 1), (5, 64, 1), (6, 64, 1)]
     rows = []
     for kind, N, iss in table:
         cyc, side, err = ctypes.c_double(), ctypes.c_double(), ctypes.c_ulonglong()
@@ -1060,10 +1123,15 @@ def run_mma_rate(args):
             continue
         M = 256 if kind == 2 else 128
         streams = iss * (2 if kind == 1 else 1)
-        per_sm_macs = 128.0 * N * 32 * streams / cyc.value  # each SM computes 128 rows per instruction
-        rows.append({"setup": names[kind], "M": M, "N": N, "issuers": iss, "cycles_per_mma": cyc.value,
-                     "int8_macs_per_sm_cycle": per_sm_macs, "frac_of_8192": per_sm_macs / 8192.0,
-                     "side_cycles_per_tmem_op": side.value if kind >= 3 else None, "wait_errors": err.value})
+        per_sm_macs = 128.0 * N * 32 * streams / cyc.value if cyc.value else None  # 128 rows per SM
+        row = {"setup": names[kind], "M": M, "N": N, "issuers": iss,
+               "cycles_per_mma": cyc.value if cyc.value else None, "int8_macs_per_sm_cycle": per_sm_macs,
+               "frac_of_8192": per_sm_macs / 8192.0 if per_sm_macs else None, "wait_errors": err.value}
+        if kind >= 3:
+            row["side_cycles_per_tmem_op"] = side.value
+            if kind in (3, 5, 6):  # 4 warps x 4 KB per store: bytes written per SM-cycle
+                row["tmem_store_bytes_per_sm_cycle"] = 4 * 4096 / side.value
+        rows.append(row)
     if rank == 0:
         print(json.dumps({"metric": "tcgen05.mma kind::i8 rate per SM (4096 back-to-back MMAs, K=32)",
                           "unit": "int8 MACs per SM-cycle", "rows": rows}), flush=True)
@@ -1080,8 +1148,10 @@ def main():
                     help="k-mers per step of the end-to-end leg (pinned host batch; 0 = all)")
     ap.add_argument("--acc-kmers", type=int, default=200_000)
     ap.add_argument("--cpu-kmers", type=int, default=1_000_000)
-    ap.add_argument("--ref-kmers", type=int, default=250_000)
+    ap.add_argument("--ref-kmers", type=int, default=500_000)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--files-kmers", type=int, default=4_000_000,
+                    help="k-mers of the pipeline-files leg of the default workload (0 = skip)")
     ap.add_argument("--no-legs", action="store_true",
                     help="default workload only: skip the FP64 n=1000/r=10 and the batched 64-phenotype legs")
     ap.add_argument("--workload", default="precision",

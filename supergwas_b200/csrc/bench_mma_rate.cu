@@ -12,7 +12,10 @@
 //   kind 3: kind 0 with one issuer while four other warps write tensor memory
 //           with tcgen05.st.32x32b.x32 (the A-operand stores of the unpack);
 //   kind 4: kind 0 with one issuer while four other warps read tensor memory
-//           with tcgen05.ld.32x32b.x16 (the accumulator loads of the epilogue).
+//           with tcgen05.ld.32x32b.x16 (the accumulator loads of the epilogue);
+//   kind 5: as kind 3, the stores issued four at a time before one
+//           tcgen05.wait::st (as the unpack warps issue them): the store rate;
+//   kind 6: kind 5 without MMAs (the issuer warp idles).
 // A comes from tensor memory (M = 128 rows, 32 bytes of K per MMA), B from
 // shared memory.  Every wait is bounded (2 s); no TMA.
 #include <cuda_runtime.h>
@@ -63,7 +66,7 @@ __global__ void __launch_bounds__(256, 512 / COLS) mma_single(unsigned long long
   tc_fence_after();
   const uint32_t tmem = s_tmem;
   unsigned long long* err = errs + (size_t)blockIdx.x * 4;
-  if (warp < ISS) {
+  if (warp < ISS && SIDE != 4) {
     const bool leader = elect_one();
     constexpr uint32_t IDESC = idesc_i8(128, N);
     const uint64_t bdesc0 = sdesc_noswz(sB, N * 16, 128);
@@ -83,16 +86,26 @@ __global__ void __launch_bounds__(256, 512 / COLS) mma_single(unsigned long long
     __syncwarp();
     if (leader) s_mma[warp] = clock64() - t0;
   } else if (SIDE && warp >= 4) {
+    constexpr int SIDE_KIND = SIDE == 4 ? 3 : SIDE;  // 4: the stores of 3 with no MMAs
     // side traffic on lane quarter (warp & 3), columns 256..287
     const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + 256;
     const unsigned long long t0 = clock64();
     unsigned long long n = 0;
-    if (SIDE == 1) {
+    if (SIDE_KIND == 1) {
       uint32_t o[32];
 #pragma unroll
       for (int k = 0; k < 32; ++k) o[k] = (uint32_t)k * 0x01010101u;
       for (int it = 0; it < kIters / 2; ++it, ++n) {
         tc_st32(taddr, o);
+        tc_wait_st();
+      }
+    } else if (SIDE_KIND == 3) {
+      uint32_t o[32];
+#pragma unroll
+      for (int k = 0; k < 32; ++k) o[k] = (uint32_t)k * 0x01010101u;
+      for (int it = 0; it < kIters / 8; ++it, n += 4) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) tc_st32(taddr + 32 * q, o);  // columns 256..383
         tc_wait_st();
       }
     } else {
@@ -228,14 +241,14 @@ int launch_and_read(K kernel, int grid, int threads, int smem, int per_cta_strea
     double mma = 0, side_ops = 0, side_cyc = 0;
     int ctas = 0;
     for (int b = 0; b < grid; ++b) {
-      if (h[4 * b] == 0) continue;  // pair kernels: the peer issues nothing
+      if (h[4 * b] == 0 && h[4 * b + 1] == 0) continue;  // pair kernels: the peer issues nothing
       mma += (double)h[4 * b];
       side_ops += (double)h[4 * b + 1];
       side_cyc += (double)h[4 * b + 2];
       r.err |= h[4 * b + 3] & 0xffffffffull;
       ++ctas;
     }
-    r.cycles_per_mma = ctas ? mma / ((double)ctas * per_cta_streams * kIters) : 0.0;
+    r.cycles_per_mma = ctas && mma > 0 ? mma / ((double)ctas * per_cta_streams * kIters) : 0.0;
     r.side_cycles_per_op = side_ops > 0 ? side_cyc / side_ops : 0.0;
     r.ok = ctas > 0 && r.err == 0;
     (void)side;
@@ -265,6 +278,11 @@ int run_kind(int kind, int issuers, int sms, Result& r) {
     case 4:
       if (N + 32 > 256) return 1;
       return launch_and_read(mma_single<N, 1, 512, 2>, sms, 256, 150 * 1024, 1, 2, r);
+    case 5:
+      if (N + 32 > 256) return 1;  // the side warps use columns 256..383
+      return launch_and_read(mma_single<N, 1, 512, 3>, sms, 256, 150 * 1024, 1, 3, r);
+    case 6:
+      return launch_and_read(mma_single<N, 1, 512, 4>, sms, 256, 150 * 1024, 1, 4, r);
     default: return 1;
   }
 }

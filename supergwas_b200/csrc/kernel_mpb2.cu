@@ -5,18 +5,19 @@
 // (HPC/kgwas/kgwas_cols.sh:22-65), i.e. the statistic of src/kgwas.cpp:44-56,
 // 132-218 once per (k-mer, phenotype).  kernel_mpb.cu runs it for every
 // phenotype in one launch with one phenotype's int8 limb image (Kpad x NP)
-// resident in shared memory per MMA group.  At r = 20+1 a phenotype has 66
-// limb columns (NP = 80), and an M = 128 kind::i8 MMA costs max(~62, N/2)
-// cycles, so N = 80 leaves 38 % of the tensor pipe idle; two phenotypes per
-// MMA (N = 160) would fill it, but their image (Kpad x 160 = 320 KB at
-// n = 2000) does not fit one SM's shared memory.
+// resident in shared memory per MMA group, and unpacks every tile's packed
+// rows into the int8 A operand once per phenotype: two phenotypes' images
+// (Kpad x 160 = 320 KB at n = 2000, r = 20+1) do not fit one SM's shared
+// memory.
 //
 // Here a cluster of two CTAs on two SMs issues M = 256 MMAs (cta_group::2):
 // each CTA holds 128 k-mers of a 256-k-mer pair-tile as its A operand in
 // tensor memory and ONE phenotype's limb image (Kpad x NP) in shared memory
 // as its half of B, and each CTA's tensor memory receives the 2 x NP
-// accumulator columns of both phenotypes for its own 128 k-mers.  Per
-// (128 k-mers, phenotype) the MMA time drops from 62 to N/4 = 40 cycles.
+// accumulator columns of both phenotypes for its own 128 k-mers.  Each tile
+// is unpacked once per two phenotypes; the MMA time per (k-mer, phenotype) is
+// the same as kernel_mpb.cu's (an M = 128 or 256 kind::i8 MMA issues N / 2
+// cycles per SM at every N measured).
 //
 // Roles (15 warps per CTA, both CTAs):
 //   0-7   epilogue, two groups of four taking pair-tile visits in turn: the
@@ -84,22 +85,17 @@ __device__ __forceinline__ uint32_t peer_addr(uint32_t local, uint32_t rank) {
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
   return r;
 }
-// Arrive on an mbarrier of any CTA of the cluster (release at cluster scope,
-// so that this CTA's tensor-memory stores are visible to the peer's MMAs).
+// Arrive on an mbarrier of any CTA of the cluster.  What the arrivals hand
+// over is tensor memory (A slots written with tcgen05.st and completed by
+// tcgen05.wait::st; accumulators read with tcgen05.ld and completed by
+// tcgen05.wait::ld) and the end of copies or MMAs, each ordered by a
+// tcgen05 fence or an mbarrier transaction, so the default (CTA-scope)
+// release of the arrive suffices: a cluster-scope release would add a
+// memory barrier to every hand-over.
 __device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
-  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+  asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
 }
-__device__ __forceinline__ bool mbar_try_cluster(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred P1;\n\t"
-      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 P1, [%1], %2, %3;\n\t"
-      "selp.b32 %0, 1, 0, P1;\n\t}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity), "r"(1000000u)
-      : "memory");
-  return ok != 0;
-}
+__device__ __forceinline__ bool mbar_try_cluster(uint32_t bar, uint32_t parity) { return mbar_try_sleep(bar, parity); }
 // Bounded wait (acquire at cluster scope) that also gives up when this CTA's
 // abort flag is raised; on giving up it raises both CTAs' flags.
 __device__ __forceinline__ bool pair_wait(uint32_t bar, uint32_t parity, volatile int* abort, uint32_t peer_abort,

@@ -106,6 +106,15 @@ def structure_basis(Xs: np.ndarray, r: int) -> np.ndarray:
     return np.ascontiguousarray(U), Ph
 
 
+def random_kmers_text(rng: np.random.Generator, m: int, k: int = 31) -> bytes:
+    """m random k-mers as the bytes of a kmers.txt file (one per line)."""
+    alph = np.frombuffer(b"ACGT", dtype=np.uint8)
+    rows = np.empty((m, k + 1), dtype=np.uint8)
+    rows[:, :k] = alph[rng.integers(0, 4, size=(m, k), dtype=np.uint8)]
+    rows[:, k] = ord("\n")
+    return rows.tobytes()
+
+
 def random_kmers(rng: np.random.Generator, m: int, k: int = 31) -> list[str]:
     alph = np.frombuffer(b"ACGT", dtype=np.uint8)
     codes = rng.integers(0, 4, size=(m, k), dtype=np.uint8)
@@ -207,21 +216,28 @@ def write_batch(dirpath: str, packed_all: np.ndarray, n_all: int, kmers,
                 gz_columns=(), kmers_plain_gz: bool = False) -> None:
     """Write a ``batch_*/`` directory: bits/col_%06d.txt[.gz] and kmers.txt.gz.
 
-    ``gz_columns`` lists sample positions whose column is written gzipped.
+    ``gz_columns`` lists sample positions whose column is written gzipped;
+    ``kmers`` is a list of strings or the bytes of the k-mer file.
     """
     os.makedirs(os.path.join(dirpath, "bits"), exist_ok=True)
-    x = unpack_rows(packed_all, n_all)  # (m, n)
     gzs = set(int(i) for i in gz_columns)
-    for j in range(n_all):
-        line = (x[:, j] + ord("0")).astype(np.uint8).tobytes() + b"\n"
-        p = os.path.join(dirpath, "bits", f"col_{j:06d}.txt")
-        if j in gzs:
-            with gzip.open(p + ".gz", "wb", compresslevel=1) as f:
-                f.write(line)
-        else:
-            with open(p, "wb") as f:
-                f.write(line)
-    data = "".join(k + "\n" for k in kmers).encode()
+    m = packed_all.shape[0]
+    # 64 samples (one packed word) at a time: their m-byte columns as rows
+    for w in range((n_all + 63) // 64):
+        bits = np.unpackbits(np.ascontiguousarray(packed_all[:, w]).view(np.uint8).reshape(m, 8), axis=1,
+                             bitorder="little")  # (m, 64)
+        cols = np.ascontiguousarray(bits.T) + np.uint8(ord("0"))
+        for t in range(min(64, n_all - 64 * w)):
+            j = 64 * w + t
+            line = cols[t].tobytes() + b"\n"
+            p = os.path.join(dirpath, "bits", f"col_{j:06d}.txt")
+            if j in gzs:
+                with gzip.open(p + ".gz", "wb", compresslevel=1) as f:
+                    f.write(line)
+            else:
+                with open(p, "wb") as f:
+                    f.write(line)
+    data = kmers if isinstance(kmers, (bytes, bytearray)) else "".join(k + "\n" for k in kmers).encode()
     kp = os.path.join(dirpath, "kmers.txt.gz")
     if kmers_plain_gz:
         with open(kp, "wb") as f:  # zlib's gzopen reads plain files transparently
