@@ -55,7 +55,7 @@ def measured_peaks():
 # k-mers it processed; the traffic grows in proportion to the k-mers, so a full
 # launch moves this many bytes per k-mer.  Capture and command:
 # profiles/ts_kernel_n1000_r16.md.
-TS_DRAM_BYTES_PER_KMER = 129.1
+TS_DRAM_BYTES_PER_KMER = 129.2
 
 
 class Clocks:
@@ -380,11 +380,10 @@ def run_ours(args):
                                     "frac": tops / (2 * bf16),
                                     "peak_note": "2x measured bf16 burst (int8 MMA issues at twice the bf16 rate)",
                                     # 16384 int8 ops per SM-cycle at the median SM clock of the timed
-                                    # region; an N=64 MMA reaches 51.6 % of it (bin/mma_rate)
+                                    # region (an N=64 MMA issues at that rate: --workload mma-rate)
                                     "hw_peak_tops_int8_at_clock": hw_peak,
                                     "frac_of_hw_peak": tops / hw_peak if hw_peak else None,
-                                    "n64_mma_ceiling_frac": 0.516,
-                                    "frac_of_n64_ceiling": tops / (0.516 * hw_peak) if hw_peak else None}},
+                                    "useful_columns": "54 of N=64 (count, 5 y' limbs, 16 x 3 U limbs)"}},
             "fp64_form": {"value": ftested / t_fp64, "unit": "k-mer tests/s", "ms_per_step": 1e3 * t_fp64,
                           "split_speedup": value / world / (ftested / t_fp64),
                           "fp64_tflops": 2.0 * m * (((n + 127) // 128) * 128) * 20 / t_fp64 / 1e12,
@@ -680,6 +679,11 @@ def run_streaming(args):
                          "peak_source": "measured (kg_probe_h2d_gbs, 8 x 1 GiB pinned)", "traffic": None},
             "kmers_per_s": kmers_per_s, "full_1e9_seconds_extrapolated": W["m_total"] / kmers_per_s,
             "chunk_seconds": chunk_s, "regen_seconds": gen_s[1:],
+            # the last chunk streams while no regeneration shares the link: the
+            # rate of kg_run_multi_host itself on 16 GB of pinned host rows
+            "last_chunk_alone": {"seconds": chunk_s[-1], "h2d_gbs": per * row / chunk_s[-1] / 1e9,
+                                 "link_frac": per * row / chunk_s[-1] / 1e9 / h2d_peak if h2d_peak else None,
+                                 "tests_per_s": tests / nchunks / chunk_s[-1]},
             "fp64_form": {"value": fp64_value, "unit": "k-mer tests/s",
                           "sample": f"{m64} device-resident k-mers x {npn} phenotypes",
                           "split_speedup": value / world / fp64_value},
