@@ -1114,10 +1114,11 @@ def run_mma_rate(args):
              3: "one CTA per SM, 4 warps storing to TMEM (one wait per store)",
              4: "one CTA per SM, 4 warps loading from TMEM",
              5: "one CTA per SM, 4 warps storing to TMEM (4 stores per wait)",
-             6: "no MMAs, 4 warps storing to TMEM (4 stores per wait)"}
+             6: "no MMAs, 4 warps storing to TMEM (4 stores per wait)",
+             7: "one CTA per SM, 4 warps reading shared memory", 8: "no MMAs, 4 warps reading shared memory"}
     table = [(0, 32, 1), (0, 64, 1), (0, 80, 1), (0, 128, 1), (0, 160, 1), (0, 256, 1), (0, 32, 2), (0, 64, 2),
              (0, 64, 4), (1, 64, 1), (2, 64, 1), (2, 128, 1), (2, 160, 1), (2, 256, 1), (3, 64, 1), (3, 128, 1),
-             (4, 64, 1), (4, 128, 1), (5, 64, 1), (6, 64, 1)]
+             (4, 64, 1), (4, 128, 1), (5, 64, 1), (6, 64, 1), (7, 64, 1), (8, 64, 1), (7, 128, 1)]
     rows = []
     for kind, N, iss in table:
         cyc, side, err = ctypes.c_double(), ctypes.c_double(), ctypes.c_ulonglong()
@@ -1135,6 +1136,8 @@ def run_mma_rate(args):
             row["side_cycles_per_tmem_op"] = side.value
             if kind in (3, 5, 6):  # 4 warps x 4 KB per store: bytes written per SM-cycle
                 row["tmem_store_bytes_per_sm_cycle"] = 4 * 4096 / side.value
+            if kind in (7, 8):     # 4 warps x 512 B per ld.shared.v4
+                row["smem_read_bytes_per_sm_cycle"] = 4 * 512 / side.value
         rows.append(row)
     if rank == 0:
         print(json.dumps({"metric": "tcgen05.mma kind::i8 rate per SM (4096 back-to-back MMAs, K=32)",

@@ -15,7 +15,11 @@
 //           with tcgen05.ld.32x32b.x16 (the accumulator loads of the epilogue);
 //   kind 5: as kind 3, the stores issued four at a time before one
 //           tcgen05.wait::st (as the unpack warps issue them): the store rate;
-//   kind 6: kind 5 without MMAs (the issuer warp idles).
+//   kind 6: kind 5 without MMAs (the issuer warp idles);
+//   kind 7: kind 0 with one issuer while four other warps read shared memory
+//           (ld.shared.v4 of the B region, as the unpack warps read row boxes):
+//           does shared-memory traffic slow the MMAs' B reads?
+//   kind 8: kind 7 without MMAs.
 // A comes from tensor memory (M = 128 rows, 32 bytes of K per MMA), B from
 // shared memory.  Every wait is bounded (2 s); no TMA.
 #include <cuda_runtime.h>
@@ -66,7 +70,7 @@ __global__ void __launch_bounds__(256, 512 / COLS) mma_single(unsigned long long
   tc_fence_after();
   const uint32_t tmem = s_tmem;
   unsigned long long* err = errs + (size_t)blockIdx.x * 4;
-  if (warp < ISS && SIDE != 4) {
+  if (warp < ISS && SIDE != 4 && SIDE != 6) {
     const bool leader = elect_one();
     constexpr uint32_t IDESC = idesc_i8(128, N);
     const uint64_t bdesc0 = sdesc_noswz(sB, N * 16, 128);
@@ -86,7 +90,7 @@ __global__ void __launch_bounds__(256, 512 / COLS) mma_single(unsigned long long
     __syncwarp();
     if (leader) s_mma[warp] = clock64() - t0;
   } else if (SIDE && warp >= 4) {
-    constexpr int SIDE_KIND = SIDE == 4 ? 3 : SIDE;  // 4: the stores of 3 with no MMAs
+    constexpr int SIDE_KIND = SIDE == 4 ? 3 : SIDE == 6 ? 5 : SIDE;  // 4, 6: kinds 3, 5 with no MMAs
     // side traffic on lane quarter (warp & 3), columns 256..287
     const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + 256;
     const unsigned long long t0 = clock64();
@@ -108,6 +112,20 @@ __global__ void __launch_bounds__(256, 512 / COLS) mma_single(unsigned long long
         for (int q = 0; q < 4; ++q) tc_st32(taddr + 32 * q, o);  // columns 256..383
         tc_wait_st();
       }
+    } else if (SIDE_KIND == 5) {
+      // 16 bytes per lane per load, 512 B per warp, walking the B region
+      uint32_t acc = 0;
+      const uint32_t span = 8 * 32 * N;
+      uint32_t off = (threadIdx.x & 127) * 16;
+      for (int it = 0; it < kIters * 2; ++it, ++n) {
+        uint32_t a0, a1, a2, a3;
+        asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(a0), "=r"(a1), "=r"(a2), "=r"(a3)
+                     : "r"(sB + off));
+        acc += a0 ^ a1 ^ a2 ^ a3;
+        off += 2048;
+        if (off >= span) off -= span;
+      }
+      if (acc == 0x12345678u) err[3] = acc;  // keeps the loads
     } else {
       uint32_t acc = 0;
       for (int it = 0; it < kIters; ++it, ++n) {
@@ -283,6 +301,8 @@ int run_kind(int kind, int issuers, int sms, Result& r) {
       return launch_and_read(mma_single<N, 1, 512, 3>, sms, 256, 150 * 1024, 1, 3, r);
     case 6:
       return launch_and_read(mma_single<N, 1, 512, 4>, sms, 256, 150 * 1024, 1, 4, r);
+    case 7: return launch_and_read(mma_single<N, 1, 512, 5>, sms, 256, 150 * 1024, 1, 5, r);
+    case 8: return launch_and_read(mma_single<N, 1, 512, 6>, sms, 256, 150 * 1024, 1, 6, r);
     default: return 1;
   }
 }

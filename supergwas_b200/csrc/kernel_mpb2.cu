@@ -551,8 +551,11 @@ static cudaError_t launch_mpb2_t(const LaunchMpb& L, const CUtensorMap& tm, cuda
   // as many pairs as can be resident at once (a GPC with an odd number of
   // free SMs leaves one SM without a partner), else a second wave of pairs
   // would double the launch
-  static int resident = -1;
-  if (resident < 0) {
+  static int resident_of[64] = {};  // per device ordinal; 0: not looked up yet
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int& resident = resident_of[dev & 63];
+  if (resident <= 0) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(L.num_sms & ~1));
     cfg.blockDim = dim3(M2_THREADS);
