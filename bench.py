@@ -1115,10 +1115,40 @@ def run_mma_rate(args):
              4: "one CTA per SM, 4 warps loading from TMEM",
              5: "one CTA per SM, 4 warps storing to TMEM (4 stores per wait)",
              6: "no MMAs, 4 warps storing to TMEM (4 stores per wait)",
-             7: "one CTA per SM, 4 warps reading shared memory", 8: "no MMAs, 4 warps reading shared memory"}
+             7: "one CTA per SM, 4 warps reading shared memory", 8: "no MMAs, 4 warps reading shared memory",
+             9: "one issuer walking A slots and the B image, a commit every 16 MMAs",
+             10: "one issuer walking A slots and the B image, a commit every 4 MMAs",
+             11: "ring of 3 A slots: 16 MMAs per use, waits for the commit of the slot's previous use",
+             12: "ring of 2 A slots: 16 MMAs per use, waits for the commit of the slot's previous use",
+             13: "ring of 3 A slots, the wait spinning on mbarrier.test_wait",
+             14: "ring of 3 A slots, the wait on try_wait with a suspend-time hint",
+             15: "ring of 3 A slots, the wait on try_wait without a hint, clock every 1024 tests",
+             16: "ring of 3 A slots, the wait spinning on test_wait, bounded by a count (no clock)",
+             17: "ring of 3 A slots, the wait on try_wait, bounded by the SM cycle counter",
+             18: "one A slot: waits for its own last commit before each use of 16 MMAs",
+             19: "ring of 3 A slots, a helper warp waiting for the commits and freeing the slots",
+             20: "ring of 3 A slots, unrolled uses with compile-time offsets after a tcgen05 fence",
+             21: "no ring: unrolled uses, a try_wait that succeeds at once before each",
+             22: "no ring: unrolled uses, two clock reads before each",
+             23: "one slot of 16 MMAs, each use after the last one's commit",
+             24: "one slot of 1 MMA, each use after the last one's commit",
+             25: "commits alone, each after the last one's arrival",
+             26: "ring of 3 slots of 16 MMAs, freed through a helper warp",
+             27: "ring of 6 slots of 8 MMAs (384 columns)",
+             28: "ring of 7 slots of 8 MMAs (448 columns)",
+             29: "ring of 7 slots of 8 MMAs, freed through a helper warp",
+             30: "ring of 3 slots of 16 MMAs (384 columns)",
+             31: "ring of 3 slots of 16 MMAs, no tcgen05 fence after the wait",
+             32: "one slot of 16 MMAs, no tcgen05 fence after the wait",
+             33: "ring of 3 slots of 16 MMAs, try_wait with a suspend-time hint"}
     table = [(0, 32, 1), (0, 64, 1), (0, 80, 1), (0, 128, 1), (0, 160, 1), (0, 256, 1), (0, 32, 2), (0, 64, 2),
              (0, 64, 4), (1, 64, 1), (2, 64, 1), (2, 128, 1), (2, 160, 1), (2, 256, 1), (3, 64, 1), (3, 128, 1),
-             (4, 64, 1), (4, 128, 1), (5, 64, 1), (6, 64, 1), (7, 64, 1), (8, 64, 1), (7, 128, 1)]
+             (4, 64, 1), (4, 128, 1), (5, 64, 1), (6, 64, 1), (7, 64, 1), (8, 64, 1), (7, 128, 1),
+             (9, 64, 1), (10, 64, 1), (11, 64, 1), (12, 64, 1), (9, 80, 1), (11, 80, 1), (11, 128, 1),
+             (13, 64, 1), (14, 64, 1), (15, 64, 1), (13, 80, 1), (14, 80, 1), (16, 64, 1), (17, 64, 1),
+             (16, 128, 1), (17, 128, 1), (18, 64, 1), (18, 128, 1), (19, 64, 1), (19, 128, 1),
+             (20, 64, 1), (21, 64, 1), (22, 64, 1), (23, 64, 1), (24, 64, 1), (25, 64, 1), (26, 64, 1),
+             (27, 64, 1), (28, 64, 1), (29, 64, 1), (30, 64, 1), (31, 64, 1), (32, 64, 1), (33, 64, 1)]
     rows = []
     for kind, N, iss in table:
         cyc, side, err = ctypes.c_double(), ctypes.c_double(), ctypes.c_ulonglong()
@@ -1132,7 +1162,11 @@ def run_mma_rate(args):
         row = {"setup": names[kind], "M": M, "N": N, "issuers": iss,
                "cycles_per_mma": cyc.value if cyc.value else None, "int8_macs_per_sm_cycle": per_sm_macs,
                "frac_of_8192": per_sm_macs / 8192.0 if per_sm_macs else None, "wait_errors": err.value}
-        if kind >= 3:
+        if 11 <= kind <= 22 and side.value:
+            row["issuer_wait_cycles_avg"] = side.value
+        if kind >= 23:
+            row["cycles_per_use"] = side.value
+        if 3 <= kind <= 8:
             row["side_cycles_per_tmem_op"] = side.value
             if kind in (3, 5, 6):  # 4 warps x 4 KB per store: bytes written per SM-cycle
                 row["tmem_store_bytes_per_sm_cycle"] = 4 * 4096 / side.value

@@ -20,6 +20,39 @@
 //           (ld.shared.v4 of the B region, as the unpack warps read row boxes):
 //           does shared-memory traffic slow the MMAs' B reads?
 //   kind 8: kind 7 without MMAs.
+//   kinds 9-12: one issuer walking the operands as the single-phenotype
+//           kernel does (A across three 128-column slots from column 128, B
+//           across 32 K-steps of the resident image for N <= 64), with a
+//           tcgen05.commit every 16 MMAs (kind 9) or every 4 (kind 10) to a
+//           barrier nobody waits on, or a ring of 3 (kind 11) or 2 (kind 12)
+//           A slots: before the MMAs of a slot's next use the issuer waits for
+//           the commit of its previous use, as the unpack warps do.  This
+//           isolates the cost of commits and of the slot hand-off from the
+//           work of the other roles.  Kinds 11 and 12 wait with mbar_wait
+//           (try_wait without a suspend-time hint, the clock read after every
+//           test); kinds 13-15 are kind 11 waiting by spinning on
+//           mbarrier.test_wait (13), on try_wait with a suspend-time hint (14)
+//           or on try_wait without one (15), the clock read every 1024 tests;
+//           kind 16 spins on test_wait bounded by a count of tests (no clock
+//           read), kind 17 on try_wait bounded by the SM cycle counter;
+//           kind 18 waits for its own last commit before each use (no ring);
+//           kind 19 is the ring of 3 with a helper warp that waits for the
+//           commits and frees the slots, the issuer waiting for the frees.
+//           kinds 20-22 issue each use as one unrolled block of 16 MMAs with
+//           compile-time offsets after a tcgen05 fence, as the kernels do:
+//           kind 20 with the ring of 3, kind 21 with a try_wait that succeeds
+//           at once before each use, kind 22 with only the clock reads.
+//           For the ring kinds the side fields give the issuer's waits and
+//           their average cycles.
+//   kinds 23-30 (mma_ring): one accumulator, A slots from column N, uses of
+//           MPU unrolled MMAs: 23 one slot of 16 MMAs (each use waits for the
+//           last: MMA time + commit latency), 24 one slot of 1 MMA, 25 commits
+//           alone, 26 three slots of 16 with a helper warp's hop, 27 six slots
+//           of 8, 28 seven slots of 8 (448 columns), 29 as 28 with the hop,
+//           30 three slots of 16 without the hop, 31 as 30 and 32 as 23
+//           without the tcgen05 fence after the wait (the probe writes no A,
+//           so nothing needs ordering), 33 as 30 waiting on try_wait with a
+//           suspend-time hint.  The side fields give cycles per use.
 // A comes from tensor memory (M = 128 rows, 32 bytes of K per MMA), B from
 // shared memory.  Every wait is bounded (2 s); no TMA.
 #include <cuda_runtime.h>
@@ -41,6 +74,39 @@ __device__ __forceinline__ uint32_t sm_id() {
   return s;
 }
 
+// Bounded wait of the ring kinds in one of three forms: WK 0 spins on
+// mbarrier.test_wait, 1 on try_wait with a suspend-time hint, 2 on try_wait
+// without one; the clock is read every 1024 tests.
+template <int WK>
+__device__ __forceinline__ bool probe_wait(uint32_t bar, uint32_t parity, unsigned long long* err) {
+  if (WK == 3) {  // test_wait, bounded by a count of tests, no clock read
+    for (uint32_t it = 0; it < (1u << 27); ++it)
+      if (mbar_test(bar, parity)) return true;
+    atomicOr(err + 2, 1ull);
+    return false;
+  }
+  if (WK == 4) {  // try_wait, bounded by the SM cycle counter
+    if (mbar_try(bar, parity)) return true;
+    const long long c0 = clock64();
+    for (uint32_t it = 1;; ++it) {
+      if (mbar_try(bar, parity)) return true;
+      if ((it & 15u) == 0 && clock64() - c0 > 4000000000ll) {
+        atomicOr(err + 2, 1ull);
+        return false;
+      }
+    }
+  }
+  const unsigned long long t0 = gtimer_ns();
+  for (uint32_t it = 1;; ++it) {
+    const bool ok = WK == 0 ? mbar_test(bar, parity) : WK == 1 ? mbar_try_sleep(bar, parity) : mbar_try(bar, parity);
+    if (ok) return true;
+    if ((it & 1023u) == 0 && gtimer_ns() - t0 > WAIT_LIMIT_NS) {
+      atomicOr(err + 2, 1ull);
+      return false;
+    }
+  }
+}
+
 // out per CTA: [0] cycles of the MMA stream(s) (sum over issuers), [1]
 // tensor-memory transfers done by the side warps, [2] their cycles, [3] error bits
 template <int N, int ISS, int COLS, int SIDE>
@@ -49,11 +115,13 @@ __global__ void __launch_bounds__(256, 512 / COLS) mma_single(unsigned long long
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   uint8_t* g = smem_raw + (base - raw);
-  const uint32_t sB = base, bars = base + 8 * 32 * N;  // B: 8 K-steps of 32 x N bytes
+  // B: KST K-steps of 32 x N bytes (32 for the walking kinds, as the kernel's image)
+  constexpr int KST = (SIDE >= 7 && N <= 64) ? 32 : 8;
+  const uint32_t sB = base, bars = base + KST * 32 * N;
   __shared__ uint32_t s_tmem;
   __shared__ unsigned long long s_mma[4];
   const int tid = threadIdx.x, warp = tid >> 5;
-  for (int i = tid; i < 8 * 32 * N / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(g)[i] = 0x01010101u * (i & 3);
+  for (int i = tid; i < KST * 32 * N / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(g)[i] = 0x01010101u * (i & 3);
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
                  "r"(COLS)
@@ -61,7 +129,7 @@ __global__ void __launch_bounds__(256, 512 / COLS) mma_single(unsigned long long
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    for (int w = 0; w < ISS; ++w) mbar_init(bars + 8 * w, 1);
+    for (int w = 0; w < 12; ++w) mbar_init(bars + 8 * w, 1);  // [0, ISS): issuers; 4..7: commits; 8..11: free slots
     mbar_fence_init();
   }
   fence_proxy_async_smem();
@@ -79,17 +147,89 @@ __global__ void __launch_bounds__(256, 512 / COLS) mma_single(unsigned long long
     const uint32_t a = tmem + ISS * N;  // 32 columns of A after the accumulators
     __syncwarp();
     const unsigned long long t0 = clock64();
-    if (leader) {
+    if (leader && SIDE < 7) {
       for (int it = 0; it < kIters; ++it) {
         const int st = it & 7;
         tc_mma_i8_ts(d, a + (st & 3) * 8, bdesc0 + st * BSTEP, IDESC, it ? 1u : 0u);
       }
       tc_commit(bars + 8 * warp);
       mbar_wait(bars + 8 * warp, 0, err, 1);
+    } else if (leader && SIDE >= 18) {
+      // per use: [SIDE 18] wait (ring of 3) + fence + 16 unrolled MMAs with
+      // compile-time offsets + commit; [19] no ring: a try_wait on a barrier
+      // whose phase 0 is already complete before each use; [20] no ring: two
+      // clock reads per use
+      const uint32_t ring = bars + 8 * 4, done0 = bars + 8 * 11;
+      if (SIDE == 19) {
+        tc_commit(done0);  // completes phase 0 once the (no) prior MMAs are done
+        mbar_wait(done0, 0, err, 1);
+      }
+      unsigned long long nwait = 0, wcyc = 0;
+      for (int su = 0; su < kIters / 16; ++su) {
+        const long long w0 = clock64();
+        if (SIDE == 18 && su >= 3) mbar_wait(ring + 8 * (su % 3), ((su / 3) - 1) & 1, err, 1);
+        if (SIDE == 19) mbar_try(done0, 0);
+        wcyc += (unsigned long long)(clock64() - w0);
+        ++nwait;
+        tc_fence_after();
+        const uint32_t a_t = tmem + 128 + (uint32_t)(su % 3) * 128;
+        const uint64_t bd = bdesc0 + (uint64_t)(((su * 16) % KST) * BSTEP);
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+          tc_mma_i8_ts(d, a_t + k * 8, bd + (uint64_t)(k * BSTEP), IDESC, (su | k) ? 1u : 0u);
+        tc_commit(ring + 8 * (su % 3));
+      }
+      tc_commit(bars + 8 * warp);
+      mbar_wait(bars + 8 * warp, 0, err, 1);
+      atomicAdd(out + (size_t)blockIdx.x * 4 + 1, nwait);
+      atomicAdd(out + (size_t)blockIdx.x * 4 + 2, wcyc);
+    } else if (leader) {
+      // 16 MMAs (512 samples) per slot use; A slot s at columns 128 + 128 s
+      constexpr int P = SIDE == 8 ? 4 : 16;          // MMAs per commit
+      // ring slots (0: no waits); SIDE 16 waits for its own last commit
+      constexpr int NS = SIDE == 16 ? 1 : (SIDE == 9 || SIDE >= 11) ? 3 : SIDE == 10 ? 2 : 0;
+      const uint32_t ring = bars + 8 * 4, freeb = bars + 8 * 8;
+      unsigned long long nwait = 0, wcyc = 0;
+      for (int it = 0; it < kIters; ++it) {
+        const int su = it / 16;  // slot use
+        if (NS && (it & 15) == 0 && su >= NS) {
+          // SIDE 17: a helper warp waits for the commits and frees the slots
+          const uint32_t rb = (SIDE == 17 ? freeb : ring) + 8 * (su % NS), rp = ((su / NS) - 1) & 1;
+          const long long w0 = clock64();
+          ++nwait;
+          if (SIDE == 11) probe_wait<0>(rb, rp, err);
+          else if (SIDE == 12) probe_wait<1>(rb, rp, err);
+          else if (SIDE == 13) probe_wait<2>(rb, rp, err);
+          else if (SIDE == 14) probe_wait<3>(rb, rp, err);
+          else if (SIDE == 15) probe_wait<4>(rb, rp, err);
+          else mbar_wait(rb, rp, err, 1);
+          wcyc += (unsigned long long)(clock64() - w0);
+        }
+        const uint32_t a_t = tmem + 128 + (uint32_t)(su % 3) * 128 + (uint32_t)(it & 15) * 8;
+        tc_mma_i8_ts(d, a_t, bdesc0 + (uint64_t)((it % KST) * BSTEP), IDESC, it ? 1u : 0u);
+        if (NS && (it & 15) == 15) tc_commit(ring + 8 * (su % NS));
+        else if (!NS && it % P == P - 1) tc_commit(ring);
+      }
+      tc_commit(bars + 8 * warp);
+      mbar_wait(bars + 8 * warp, 0, err, 1);
+      if (NS) {  // waits of the issuer: count and cycles
+        atomicAdd(out + (size_t)blockIdx.x * 4 + 1, nwait);
+        atomicAdd(out + (size_t)blockIdx.x * 4 + 2, wcyc);
+      }
     }
     __syncwarp();
     if (leader) s_mma[warp] = clock64() - t0;
-  } else if (SIDE && warp >= 4) {
+  } else if (SIDE == 17 && warp == 4) {
+    // helper: waits for each use's commit in order and frees its slot
+    if (elect_one()) {
+      const uint32_t ring = bars + 8 * 4, freeb = bars + 8 * 8;
+      for (int su = 0; su < kIters / 16; ++su) {
+        if (!mbar_wait(ring + 8 * (su % 3), (su / 3) & 1, err, 1)) break;
+        mbar_arrive(freeb + 8 * (su % 3));
+      }
+    }
+    __syncwarp();
+  } else if (SIDE && SIDE <= 6 && warp >= 4) {
     constexpr int SIDE_KIND = SIDE == 4 ? 3 : SIDE == 6 ? 5 : SIDE;  // 4, 6: kinds 3, 5 with no MMAs
     // side traffic on lane quarter (warp & 3), columns 256..287
     const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + 256;
@@ -119,7 +259,9 @@ __global__ void __launch_bounds__(256, 512 / COLS) mma_single(unsigned long long
       uint32_t off = (threadIdx.x & 127) * 16;
       for (int it = 0; it < kIters * 2; ++it, ++n) {
         uint32_t a0, a1, a2, a3;
-        asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(a0), "=r"(a1), "=r"(a2), "=r"(a3)
+        // volatile: the addresses repeat every 8 loads and nothing stores to
+        // them, so plain loads could be merged by the compiler
+        asm volatile("ld.volatile.shared.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(a0), "=r"(a1), "=r"(a2), "=r"(a3)
                      : "r"(sB + off));
         acc += a0 ^ a1 ^ a2 ^ a3;
         off += 2048;
@@ -152,6 +294,98 @@ __global__ void __launch_bounds__(256, 512 / COLS) mma_single(unsigned long long
   }
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(COLS) : "memory");
+}
+
+// Ring of NSL A slots of MPU MMAs each (A from column N, one accumulator at
+// column 0), the uses issued as unrolled blocks with compile-time offsets.
+// Before a slot's next use the issuer waits for the commit of its previous
+// use (HOP = 0), or for a helper warp that waits for that commit and then
+// arrives on a second barrier (HOP = 1: the hand-off through another role).
+// MPU = 0: commits only (the round trip of a commit with no MMA behind it).
+// out[0]: cycles of the issuer; [1] uses, [2] the same cycles (cycles per use).
+template <int N, int NSL, int MPU, int HOP, int FENCE = 1>
+__global__ void __launch_bounds__(256, 1) mma_ring(unsigned long long* out, unsigned long long* errs) {
+  constexpr int KST = N <= 64 ? 32 : 8;
+  constexpr int USES = MPU ? kIters / MPU : 256;
+  static_assert(N > 64 || N + NSL * (MPU ? MPU : 1) * 8 <= 512, "TMEM columns");  // launched for N <= 64
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t* g = smem_raw + (base - raw);
+  const uint32_t sB = base, commitb = base + KST * 32 * N, freeb = commitb + 8 * 8, fin = freeb + 8 * 8;
+  __shared__ uint32_t s_tmem;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int i = tid; i < KST * 32 * N / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(g)[i] = 0x01010101u * (i & 3);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&s_tmem))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int w = 0; w < 17; ++w) mbar_init(commitb + 8 * w, 1);
+    mbar_fence_init();
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  unsigned long long* err = errs + (size_t)blockIdx.x * 4;
+  if (warp == 0) {
+    const bool leader = elect_one();
+    constexpr uint32_t IDESC = idesc_i8(128, N);
+    const uint64_t bdesc0 = sdesc_noswz(sB, N * 16, 128);
+    constexpr uint32_t BSTEP = (2 * N * 16) >> 4;
+    __syncwarp();
+    const unsigned long long t0 = clock64();
+    if (leader) {
+      unsigned long long wcyc = 0;
+      for (int su = 0; su < USES; ++su) {
+        const int slot = su % NSL;
+        if (su >= NSL) {
+          const long long w0 = clock64();
+          if (HOP == 2) {  // try_wait with a suspend-time hint
+            const uint32_t rb = commitb + 8 * slot, rp = ((su / NSL) - 1) & 1;
+            while (!mbar_try_sleep(rb, rp)) {
+            }
+          } else {
+            mbar_wait((HOP ? freeb : commitb) + 8 * slot, ((su / NSL) - 1) & 1, err, 1);
+          }
+          wcyc += (unsigned long long)(clock64() - w0);
+        }
+        if (FENCE) tc_fence_after();
+        if (MPU) {
+          const uint32_t a_t = tmem + N + (uint32_t)slot * (MPU * 8);
+          const uint64_t bd = bdesc0 + (uint64_t)(((su * MPU) % KST) * BSTEP);
+#pragma unroll
+          for (int k = 0; k < MPU; ++k)
+            tc_mma_i8_ts(tmem, a_t + k * 8, bd + (uint64_t)((k % KST) * BSTEP), IDESC, (su | k) ? 1u : 0u);
+        }
+        tc_commit(commitb + 8 * slot);
+      }
+      tc_commit(fin);
+      mbar_wait(fin, 0, err, 1);
+      const unsigned long long tot = clock64() - t0;
+      out[(size_t)blockIdx.x * 4] = tot;
+      out[(size_t)blockIdx.x * 4 + 1] = USES;
+      out[(size_t)blockIdx.x * 4 + 2] = tot;
+      (void)wcyc;
+    }
+    __syncwarp();
+  } else if (HOP == 1 && warp == 1) {
+    if (elect_one()) {
+      for (int su = 0; su < USES; ++su) {
+        if (!mbar_wait(commitb + 8 * (su % NSL), (su / NSL) & 1, err, 1)) break;
+        mbar_arrive(freeb + 8 * (su % NSL));
+      }
+    }
+    __syncwarp();
+  }
+  if (tid == 0) out[(size_t)blockIdx.x * 4 + 3] = err[2];
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
 }
 
 __device__ __forceinline__ uint32_t cluster_rank() {
@@ -303,6 +537,32 @@ int run_kind(int kind, int issuers, int sms, Result& r) {
       return launch_and_read(mma_single<N, 1, 512, 4>, sms, 256, 150 * 1024, 1, 4, r);
     case 7: return launch_and_read(mma_single<N, 1, 512, 5>, sms, 256, 150 * 1024, 1, 5, r);
     case 8: return launch_and_read(mma_single<N, 1, 512, 6>, sms, 256, 150 * 1024, 1, 6, r);
+    // kinds 9-12: accumulator + three 128-column A slots from column 128
+    case 9: return N > 128 ? 1 : launch_and_read(mma_single<N, 1, 512, 7>, sms, 256, 150 * 1024, 1, 0, r);
+    case 10: return N > 128 ? 1 : launch_and_read(mma_single<N, 1, 512, 8>, sms, 256, 150 * 1024, 1, 0, r);
+    case 11: return N > 128 ? 1 : launch_and_read(mma_single<N, 1, 512, 9>, sms, 256, 150 * 1024, 1, 0, r);
+    case 12: return N > 128 ? 1 : launch_and_read(mma_single<N, 1, 512, 10>, sms, 256, 150 * 1024, 1, 0, r);
+    case 13: return N > 128 ? 1 : launch_and_read(mma_single<N, 1, 512, 11>, sms, 256, 150 * 1024, 1, 0, r);
+    case 14: return N > 128 ? 1 : launch_and_read(mma_single<N, 1, 512, 12>, sms, 256, 150 * 1024, 1, 0, r);
+    case 15: return N > 128 ? 1 : launch_and_read(mma_single<N, 1, 512, 13>, sms, 256, 150 * 1024, 1, 0, r);
+    case 16: return N > 128 ? 1 : launch_and_read(mma_single<N, 1, 512, 14>, sms, 256, 150 * 1024, 1, 0, r);
+    case 17: return N > 128 ? 1 : launch_and_read(mma_single<N, 1, 512, 15>, sms, 256, 150 * 1024, 1, 0, r);
+    case 18: return N > 128 ? 1 : launch_and_read(mma_single<N, 1, 512, 16>, sms, 256, 150 * 1024, 1, 0, r);
+    case 19: return N > 128 ? 1 : launch_and_read(mma_single<N, 1, 512, 17>, sms, 256, 150 * 1024, 1, 0, r);
+    case 20: return N > 64 ? 1 : launch_and_read(mma_single<N, 1, 512, 18>, sms, 256, 150 * 1024, 1, 0, r);
+    case 21: return N > 64 ? 1 : launch_and_read(mma_single<N, 1, 512, 19>, sms, 256, 150 * 1024, 1, 0, r);
+    case 22: return N > 64 ? 1 : launch_and_read(mma_single<N, 1, 512, 20>, sms, 256, 150 * 1024, 1, 0, r);
+    case 23: return N > 64 ? 1 : launch_and_read(mma_ring<N, 1, 16, 0>, sms, 256, 150 * 1024, 1, 0, r);
+    case 24: return N > 64 ? 1 : launch_and_read(mma_ring<N, 1, 1, 0>, sms, 256, 150 * 1024, 1, 0, r);
+    case 25: return N > 64 ? 1 : launch_and_read(mma_ring<N, 1, 0, 0>, sms, 256, 150 * 1024, 1, 0, r);
+    case 26: return N > 64 ? 1 : launch_and_read(mma_ring<N, 3, 16, 1>, sms, 256, 150 * 1024, 1, 0, r);
+    case 27: return N > 64 ? 1 : launch_and_read(mma_ring<N, 6, 8, 0>, sms, 256, 150 * 1024, 1, 0, r);
+    case 28: return N > 64 ? 1 : launch_and_read(mma_ring<N, 7, 8, 0>, sms, 256, 150 * 1024, 1, 0, r);
+    case 29: return N > 64 ? 1 : launch_and_read(mma_ring<N, 7, 8, 1>, sms, 256, 150 * 1024, 1, 0, r);
+    case 30: return N > 64 ? 1 : launch_and_read(mma_ring<N, 3, 16, 0>, sms, 256, 150 * 1024, 1, 0, r);
+    case 31: return N > 64 ? 1 : launch_and_read(mma_ring<N, 3, 16, 0, 0>, sms, 256, 150 * 1024, 1, 0, r);
+    case 32: return N > 64 ? 1 : launch_and_read(mma_ring<N, 1, 16, 0, 0>, sms, 256, 150 * 1024, 1, 0, r);
+    case 33: return N > 64 ? 1 : launch_and_read(mma_ring<N, 3, 16, 2>, sms, 256, 150 * 1024, 1, 0, r);
     default: return 1;
   }
 }
