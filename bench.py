@@ -1140,7 +1140,36 @@ def run_mma_rate(args):
              30: "ring of 3 slots of 16 MMAs (384 columns)",
              31: "ring of 3 slots of 16 MMAs, no tcgen05 fence after the wait",
              32: "one slot of 16 MMAs, no tcgen05 fence after the wait",
-             33: "ring of 3 slots of 16 MMAs, try_wait with a suspend-time hint"}
+             33: "ring of 3 slots of 16 MMAs, try_wait with a suspend-time hint",
+             34: "ring of 3 slots of 16 MMAs, the next slot waited for before the commit",
+             35: "ring of 2 slots of 16 MMAs, the next slot waited for before the commit",
+             36: "ring of 6 slots of 8 MMAs, the next slot waited for before the commit",
+             37: "ring of 3 slots of 16 MMAs, 7 other warps spinning on try_wait",
+             38: "ring of 3 slots of 16 MMAs, 7 other warps on try_wait with a suspend-time hint",
+             39: "ring of 3 slots of 16 MMAs, 7 other warps sleeping 128 ns between tries",
+             40: "kernel-shaped ring (576 threads, issuer warp 17, warp-wide waits)",
+             41: "kernel-shaped ring, two accumulators alternating by tile",
+             42: "kernel-shaped ring, two accumulators with the epilogue hand-off",
+             43: "kernel-shaped ring, slots freed through a group of four warps",
+             44: "kernel-shaped ring, accumulator and slot hand-offs",
+             45: "as 44, one thread waiting at the top of each use",
+             46: "as 45, the accumulator waited for one use earlier",
+             47: "as 44, one thread waiting for the next use's barriers after 8 of 16 MMAs",
+             48: "as 44, one thread testing after 8 of 16 MMAs, waiting after the commits only on a miss",
+             49: "as 43, one thread waiting at the top of each use",
+             50: "as 43, one thread waiting after 8 of 16 MMAs",
+             51: "as 44, eight other warps doing integer work (2 chains)",
+             52: "as 47, eight other warps doing integer work (2 chains)",
+             53: "as 44, eight other warps doing integer work (4 chains)",
+             54: "as 47, eight other warps doing integer work (4 chains)",
+             55: "as 44 with two issuers taking alternate tiles",
+             56: "as 55, eight other warps doing integer work (2 chains)",
+             57: "as 55, eight other warps doing integer work (4 chains)",
+             58: "two issuers, private rings of 3 slots of 8 MMAs",
+             59: "two issuers, private rings of 2 slots of 8 MMAs",
+             60: "two issuers, private rings of 1 slot of 16 MMAs",
+             61: "as 55, eight other warps running FP64 multiply-add chains",
+             62: "as 44, eight other warps running FP64 multiply-add chains"}
     table = [(0, 32, 1), (0, 64, 1), (0, 80, 1), (0, 128, 1), (0, 160, 1), (0, 256, 1), (0, 32, 2), (0, 64, 2),
              (0, 64, 4), (1, 64, 1), (2, 64, 1), (2, 128, 1), (2, 160, 1), (2, 256, 1), (3, 64, 1), (3, 128, 1),
              (4, 64, 1), (4, 128, 1), (5, 64, 1), (6, 64, 1), (7, 64, 1), (8, 64, 1), (7, 128, 1),
@@ -1148,7 +1177,12 @@ def run_mma_rate(args):
              (13, 64, 1), (14, 64, 1), (15, 64, 1), (13, 80, 1), (14, 80, 1), (16, 64, 1), (17, 64, 1),
              (16, 128, 1), (17, 128, 1), (18, 64, 1), (18, 128, 1), (19, 64, 1), (19, 128, 1),
              (20, 64, 1), (21, 64, 1), (22, 64, 1), (23, 64, 1), (24, 64, 1), (25, 64, 1), (26, 64, 1),
-             (27, 64, 1), (28, 64, 1), (29, 64, 1), (30, 64, 1), (31, 64, 1), (32, 64, 1), (33, 64, 1)]
+             (27, 64, 1), (28, 64, 1), (29, 64, 1), (30, 64, 1), (31, 64, 1), (32, 64, 1), (33, 64, 1),
+             (34, 64, 1), (35, 64, 1), (36, 64, 1), (37, 64, 1), (38, 64, 1), (39, 64, 1),
+             (40, 64, 1), (41, 64, 1), (42, 64, 1), (43, 64, 1), (44, 64, 1), (45, 64, 1), (46, 64, 1),
+             (47, 64, 1), (48, 64, 1), (49, 64, 1), (50, 64, 1), (51, 64, 1), (52, 64, 1), (53, 64, 1),
+             (54, 64, 1), (55, 64, 1), (56, 64, 1), (57, 64, 1), (58, 64, 1), (59, 64, 1), (60, 64, 1), (61, 64, 1),
+             (62, 64, 1)]
     rows = []
     for kind, N, iss in table:
         cyc, side, err = ctypes.c_double(), ctypes.c_double(), ctypes.c_ulonglong()
@@ -1173,9 +1207,31 @@ def run_mma_rate(args):
             if kind in (7, 8):     # 4 warps x 512 B per ld.shared.v4
                 row["smem_read_bytes_per_sm_cycle"] = 4 * 512 / side.value
         rows.append(row)
+    # timeline of one issuer on a ring of A slots: how long a use takes to
+    # issue (queue back-pressure) and how long the wait for its slot takes
+    L.kg_bench_mma_timeline.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong)]
+    timelines = []
+    forms = {0: "with a disable-output-lane mask", 1: "no mask", 2: "no mask, constant accumulate predicate"}
+    for nsl, form in ((1, 0), (2, 0), (3, 0), (1, 1), (3, 1), (1, 2), (3, 2), (4, 0)):
+        buf = (ctypes.c_ulonglong * (3 * 256))()
+        rc = L.kg_bench_mma_timeline(nsl, form, buf)
+        if rc != 0:
+            timelines.append({"slots": nsl, "form": form, "rc": rc})
+            continue
+        t = [buf[i] for i in range(3 * 256)]
+        nuse = 4096 // 48 if nsl == 4 else 256
+        uses = range(4 if nsl == 4 else 16, nuse)  # steady state
+        wait = [t[3 * u + 1] - t[3 * u] for u in uses]
+        issue = [t[3 * u + 2] - t[3 * u + 1] for u in uses]
+        period = (t[3 * (nuse - 1) + 2] - t[3 * uses[0] + 2]) / (nuse - 1 - uses[0])
+        timelines.append({"slots": 1 if nsl == 4 else nsl, "mmas_per_use": 48 if nsl == 4 else 16,
+                          "form": forms[form], "cycles_per_use": period,
+                          "wait_cycles_avg": sum(wait) / len(wait), "wait_cycles_max": max(wait),
+                          "issue_cycles_avg": sum(issue) / len(issue), "issue_cycles_max": max(issue),
+                          "first_uses": [[t[3 * u], t[3 * u + 1], t[3 * u + 2]] for u in range(8)]})
     if rank == 0:
         print(json.dumps({"metric": "tcgen05.mma kind::i8 rate per SM (4096 back-to-back MMAs, K=32)",
-                          "unit": "int8 MACs per SM-cycle", "rows": rows}), flush=True)
+                          "unit": "int8 MACs per SM-cycle", "rows": rows, "ring_timelines": timelines}), flush=True)
 
 
 def main():

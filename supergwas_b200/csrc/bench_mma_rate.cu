@@ -52,7 +52,32 @@
 //           30 three slots of 16 without the hop, 31 as 30 and 32 as 23
 //           without the tcgen05 fence after the wait (the probe writes no A,
 //           so nothing needs ordering), 33 as 30 waiting on try_wait with a
-//           suspend-time hint.  The side fields give cycles per use.
+//           suspend-time hint; 34-36 (rings of 3 x 16, 2 x 16, 6 x 8) wait
+//           for the next use's slot after issuing a use's MMAs and before
+//           committing them, so no wait lies between a commit and the next
+//           MMA; 37-39 are kind 30 while the CTA's seven other warps wait on
+//           a barrier that never completes (try_wait; with a suspend-time
+//           hint; after a 128 ns sleep), as a kernel's other roles wait.
+//           The side fields give cycles per use.
+//   kinds 40-44 (mma_pipe, 576 threads, the issuer in warp 17): the ring of
+//           3 x 16 as the single-phenotype kernel runs it, its features added
+//           one at a time: 40 none, 41 two accumulators alternating by tile,
+//           42 + the accumulator hand-off through an epilogue group, 43 the
+//           slot hand-off through a group of four warps, 44 all of them;
+//           45-48 are kind 44 with one thread waiting: at the top of each use
+//           (45), with the accumulator one use earlier (46), in the middle of
+//           the previous use's MMAs (47), or testing there and waiting after
+//           the commits only if a test failed (48); 49, 50 are kind 43 (no
+//           accumulator hand-off) waiting as 45 and 47; 51-54 are kinds 44
+//           and 47 while eight other warps (two per sub-partition) do
+//           integer work with 2 (51, 52) or 4 (53, 54) independent chains;
+//           55-57: two issuers (warps 16, 17) taking alternate tiles, each
+//           with its own accumulator, alone (55) and beside the busy warps
+//           with 2 (56) or 4 (57) chains;
+//   kinds 58-60 (mma_pipe2): two issuers with private rings, their own
+//           slot and accumulator groups: 3 slots of 8 MMAs each (58), 2 of 8
+//           (59), 1 of 16 (60); 61, 62: kinds 56 and 51 with the eight
+//           busy warps running FP64 multiply-add chains.
 // A comes from tensor memory (M = 128 rows, 32 bytes of K per MMA), B from
 // shared memory.  Every wait is bounded (2 s); no TMA.
 #include <cuda_runtime.h>
@@ -303,7 +328,7 @@ __global__ void __launch_bounds__(256, 512 / COLS) mma_single(unsigned long long
 // arrives on a second barrier (HOP = 1: the hand-off through another role).
 // MPU = 0: commits only (the round trip of a commit with no MMA behind it).
 // out[0]: cycles of the issuer; [1] uses, [2] the same cycles (cycles per use).
-template <int N, int NSL, int MPU, int HOP, int FENCE = 1>
+template <int N, int NSL, int MPU, int HOP, int FENCE = 1, int ORDER = 0, int SPIN = 0>
 __global__ void __launch_bounds__(256, 1) mma_ring(unsigned long long* out, unsigned long long* errs) {
   constexpr int KST = N <= 64 ? 32 : 8;
   constexpr int USES = MPU ? kIters / MPU : 256;
@@ -314,6 +339,7 @@ __global__ void __launch_bounds__(256, 1) mma_ring(unsigned long long* out, unsi
   uint8_t* g = smem_raw + (base - raw);
   const uint32_t sB = base, commitb = base + KST * 32 * N, freeb = commitb + 8 * 8, fin = freeb + 8 * 8;
   __shared__ uint32_t s_tmem;
+  __shared__ volatile int s_done;
   const int tid = threadIdx.x, warp = tid >> 5;
   for (int i = tid; i < KST * 32 * N / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(g)[i] = 0x01010101u * (i & 3);
   if (warp == 0) {
@@ -322,8 +348,9 @@ __global__ void __launch_bounds__(256, 1) mma_ring(unsigned long long* out, unsi
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    for (int w = 0; w < 17; ++w) mbar_init(commitb + 8 * w, 1);
+    for (int w = 0; w < 18; ++w) mbar_init(commitb + 8 * w, 1);  // the last: never completed (spinners)
     mbar_fence_init();
+    s_done = 0;
   }
   fence_proxy_async_smem();
   tc_fence_before();
@@ -342,6 +369,19 @@ __global__ void __launch_bounds__(256, 1) mma_ring(unsigned long long* out, unsi
       unsigned long long wcyc = 0;
       for (int su = 0; su < USES; ++su) {
         const int slot = su % NSL;
+        if (ORDER == 1) {
+          // this use's slot was waited for before the last commit
+          if (FENCE) tc_fence_after();
+          const uint32_t a_t = tmem + N + (uint32_t)slot * (MPU * 8);
+          const uint64_t bd = bdesc0 + (uint64_t)(((su * MPU) % KST) * BSTEP);
+#pragma unroll
+          for (int k = 0; k < MPU; ++k)
+            tc_mma_i8_ts(tmem, a_t + k * 8, bd + (uint64_t)((k % KST) * BSTEP), IDESC, (su | k) ? 1u : 0u);
+          const int nx = su + 1;
+          if (nx < USES && nx >= NSL) mbar_wait(commitb + 8 * (nx % NSL), ((nx / NSL) - 1) & 1, err, 1);
+          tc_commit(commitb + 8 * slot);
+          continue;
+        }
         if (su >= NSL) {
           const long long w0 = clock64();
           if (HOP == 2) {  // try_wait with a suspend-time hint
@@ -366,12 +406,23 @@ __global__ void __launch_bounds__(256, 1) mma_ring(unsigned long long* out, unsi
       tc_commit(fin);
       mbar_wait(fin, 0, err, 1);
       const unsigned long long tot = clock64() - t0;
+      s_done = 1;
       out[(size_t)blockIdx.x * 4] = tot;
       out[(size_t)blockIdx.x * 4 + 1] = USES;
       out[(size_t)blockIdx.x * 4 + 2] = tot;
       (void)wcyc;
     }
     __syncwarp();
+  } else if (SPIN && warp >= 1) {
+    // warps waiting on a barrier that never completes, as the other roles of
+    // a kernel wait for theirs: SPIN 1 try_wait, 2 try_wait with a
+    // suspend-time hint, 3 try_wait after a 128 ns sleep; bounded by a count
+    const uint32_t never = commitb + 8 * 17;
+    for (uint32_t it = 0; it < (1u << 22) && !s_done; ++it) {
+      if (SPIN == 3) __nanosleep(128);
+      const bool r = SPIN == 2 ? mbar_try_sleep(never, 0) : mbar_try(never, 0);
+      if (r) break;
+    }
   } else if (HOP == 1 && warp == 1) {
     if (elect_one()) {
       for (int su = 0; su < USES; ++su) {
@@ -380,6 +431,411 @@ __global__ void __launch_bounds__(256, 1) mma_ring(unsigned long long* out, unsi
       }
     }
     __syncwarp();
+  }
+  if (tid == 0) out[(size_t)blockIdx.x * 4 + 3] = err[2];
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+}
+
+// Timeline of one issuer (CTA 0) on a ring of NSL A slots of 16 MMAs, N = 64:
+// per use, the clock when its wait began, when the wait returned and when
+// its last MMA and commit had been issued.  tl: 3 * kIters / 16 values.
+// FORM 0: the association kernels' MMA (disable-output-lane mask of four
+// zero registers, predicate from a register); 1: no mask; 2: no mask and a
+// constant accumulate predicate after the first MMA.
+template <int FORM>
+__device__ __forceinline__ void mma_form(uint32_t d, uint32_t a, uint64_t bd, uint32_t idesc, uint32_t acc) {
+  if (FORM == 0) {
+    tc_mma_i8_ts(d, a, bd, idesc, acc);
+  } else if (FORM == 1 || acc == 0) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d),
+        "r"(a), "l"(bd), "r"(idesc), "r"(acc)
+        : "memory");
+  } else {
+    asm volatile("tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, 1;" ::"r"(d), "r"(a), "l"(bd), "r"(idesc)
+                 : "memory");
+  }
+}
+
+template <int NSL, int FORM = 0, int MPU = 16>
+__global__ void __launch_bounds__(128, 1) mma_ring_timeline(unsigned long long* tl, unsigned long long* errs) {
+  constexpr int N = 64, KST = 32, USES = kIters / MPU;
+  static_assert(MPU % 16 == 0 && NSL * MPU * 8 + 64 <= 512, "TMEM columns");
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t* g = smem_raw + (base - raw);
+  const uint32_t sB = base, commitb = base + KST * 32 * N, fin = commitb + 8 * 8;
+  __shared__ uint32_t s_tmem;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int i = tid; i < KST * 32 * N / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(g)[i] = 0x01010101u * (i & 3);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&s_tmem))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int w = 0; w < 9; ++w) mbar_init(commitb + 8 * w, 1);
+    mbar_fence_init();
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  unsigned long long* err = errs + (size_t)blockIdx.x * 4;
+  if (warp == 0) {
+    const bool leader = elect_one();
+    constexpr uint32_t IDESC = idesc_i8(128, N);
+    const uint64_t bdesc0 = sdesc_noswz(sB, N * 16, 128);
+    constexpr uint32_t BSTEP = (2 * N * 16) >> 4;
+    __syncwarp();
+    if (leader) {
+      const long long t0 = clock64();
+      for (int su = 0; su < USES; ++su) {
+        const int slot = su % NSL;
+        const long long a = clock64();
+        if (su >= NSL) mbar_wait(commitb + 8 * slot, ((su / NSL) - 1) & 1, err, 1);
+        const long long b = clock64();
+        tc_fence_after();
+        const uint32_t a_t = tmem + N + (uint32_t)slot * (MPU * 8);
+#pragma unroll
+        for (int k = 0; k < MPU; ++k)
+          mma_form<FORM>(tmem, a_t + k * 8, bdesc0 + (uint64_t)((k % KST) * BSTEP), IDESC, (su | k) ? 1u : 0u);
+        tc_commit(commitb + 8 * slot);
+        const long long c = clock64();
+        if (blockIdx.x == 0) {
+          tl[3 * su] = (unsigned long long)(a - t0);
+          tl[3 * su + 1] = (unsigned long long)(b - t0);
+          tl[3 * su + 2] = (unsigned long long)(c - t0);
+        }
+      }
+      tc_commit(fin);
+      mbar_wait(fin, 0, err, 1);
+    }
+    __syncwarp();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+}
+
+// The single-phenotype kernel's MMA pipeline rebuilt step by step (N = 64,
+// three A slots of 16 MMAs, tiles of two slot uses): ACC2 alternates two
+// accumulators tile by tile (the first MMA of a tile overwrites); ACCW adds
+// the accumulator hand-off (a commit per tile that an "epilogue" group of
+// four warps waits for, and its release that the issuer waits for before
+// reusing the buffer); HOPW frees the A slots through a group of four warps
+// (each waits for the commit, the slot counts four arrivals) that the issuer
+// waits for, instead of waiting for the commit itself.  out[0]: the issuer's
+// cycles; [1] uses, [2] the same cycles.
+template <int ACC2, int ACCW, int HOPW, int MODE = 0, int BUSY = 0, int ISS2 = 0>
+__global__ void __launch_bounds__(576, 1) mma_pipe(unsigned long long* out, unsigned long long* errs) {
+  constexpr int N = 64, KST = 32, USES = kIters / 16, NSL = 3;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t* g = smem_raw + (base - raw);
+  const uint32_t sB = base, a_empty = base + KST * 32 * N, a_full = a_empty + 32, acc_full = a_full + 32,
+                 acc_empty = acc_full + 16, fin = acc_empty + 16;
+  __shared__ uint32_t s_tmem;
+  __shared__ volatile int s_stop;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < KST * 32 * N / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(g)[i] = 0x01010101u * (i & 3);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&s_tmem))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    s_stop = 0;
+    for (int t = 0; t < NSL; ++t) mbar_init(a_empty + 8 * t, 1), mbar_init(a_full + 8 * t, 4);
+    for (int t = 0; t < 2; ++t) mbar_init(acc_full + 8 * t, 1), mbar_init(acc_empty + 8 * t, 4);
+    mbar_init(fin, 1);
+    mbar_init(fin + 8, 1);
+    mbar_fence_init();
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  unsigned long long* err = errs + (size_t)blockIdx.x * 4;
+  if (ISS2 && (warp == 16 || warp == 17)) {
+    // two issuers on two sub-partitions, taking alternate tiles (issuer j:
+    // tiles t with t % 2 == j, accumulator j); one thread each, waiting at
+    // the top of each use
+    const int j = warp - 16;
+    const bool leader = elect_one();
+    constexpr uint32_t IDESC = idesc_i8(128, N);
+    const uint64_t bdesc0 = sdesc_noswz(sB, N * 16, 128);
+    constexpr uint32_t BSTEP = (2 * N * 16) >> 4;
+    __syncwarp();
+    const unsigned long long t0 = clock64();
+    if (leader) {
+      for (int tile = j; tile < USES / 2; tile += 2) {
+        if (tile >= 2) mbar_wait(acc_empty + 8 * j, ((tile >> 1) - 1) & 1, err, 1);
+        for (int u = 0; u < 2; ++u) {
+          const int su = 2 * tile + u, slot = su % NSL;
+          if (su >= NSL) mbar_wait(a_full + 8 * slot, ((su / NSL) - 1) & 1, err, 1);
+          tc_fence_after();
+          const uint32_t a_t = tmem + 2 * N + (uint32_t)slot * 128;
+          const uint32_t d_t = tmem + j * N;
+          const uint64_t bd = bdesc0 + (uint64_t)(((su * 16) % KST) * BSTEP);
+#pragma unroll
+          for (int k = 0; k < 16; ++k)
+            tc_mma_i8_ts(d_t, a_t + k * 8, bd + (uint64_t)(k * BSTEP), IDESC, (u | k) ? 1u : 0u);
+          tc_commit(a_empty + 8 * slot);
+        }
+        tc_commit(acc_full + 8 * j);
+      }
+      tc_commit(fin + 8 * j);
+      mbar_wait(fin + 8 * j, 0, err, 1);
+      const unsigned long long tot = clock64() - t0;
+      if (j == 1) s_stop = 1;
+      atomicMax(out + (size_t)blockIdx.x * 4, tot);
+      out[(size_t)blockIdx.x * 4 + 1] = USES;
+      atomicMax(out + (size_t)blockIdx.x * 4 + 2, tot);
+    }
+    __syncwarp();
+  } else if (!ISS2 && warp == 17) {
+    // issuer (the kernel's MMA warp is warp 17)
+    const bool leader = elect_one();
+    constexpr uint32_t IDESC = idesc_i8(128, N);
+    const uint64_t bdesc0 = sdesc_noswz(sB, N * 16, 128);
+    constexpr uint32_t BSTEP = (2 * N * 16) >> 4;
+    const unsigned long long t0 = clock64();
+    const uint32_t slot_bar = HOPW ? a_full : a_empty;
+    if (MODE >= 1 && leader) {
+      // one thread: MODE 1 waits at the top of each use; 2 as 1 with a tile's
+      // accumulator waited for one use earlier; 3 waits for what the next use
+      // needs after 8 of this use's 16 MMAs; 4 only tests there
+      // (mbarrier.test_wait) and waits after the commits if a test failed
+      for (int su = 0; su < USES; ++su) {
+        const int slot = su % NSL, tile = su >> 1, b = ACC2 ? (tile & 1) : 0;
+        if (MODE == 1) {
+          if (ACCW && (su & 1) == 0 && tile >= 2) mbar_wait(acc_empty + 8 * b, ((tile >> 1) - 1) & 1, err, 1);
+          if (su >= NSL) mbar_wait(slot_bar + 8 * slot, ((su / NSL) - 1) & 1, err, 1);
+        } else if (MODE == 2) {
+          if (su >= NSL) mbar_wait(slot_bar + 8 * slot, ((su / NSL) - 1) & 1, err, 1);
+          if (ACCW && (su & 1) == 1 && tile + 1 >= 2)
+            mbar_wait(acc_empty + 8 * (b ^ 1), (((tile + 1) >> 1) - 1) & 1, err, 1);
+        }
+        tc_fence_after();
+        const uint32_t a_t = tmem + 2 * N + (uint32_t)slot * 128;
+        const uint32_t d_t = tmem + b * N;
+        const uint64_t bd = bdesc0 + (uint64_t)(((su * 16) % KST) * BSTEP);
+        const uint32_t first = ACC2 ? (su & 1) : su;
+        const int nx = su + 1, nslot = nx % NSL, ntile = nx >> 1, nb = ACC2 ? (ntile & 1) : 0;
+        const bool need_slot = nx < USES && nx >= NSL;
+        const bool need_acc = ACCW && nx < USES && (nx & 1) == 0 && ntile >= 2;
+        bool slot_ok = true, acc_ok = true;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          if (k == 8 && MODE == 3) {
+            if (need_slot) mbar_wait(slot_bar + 8 * nslot, ((nx / NSL) - 1) & 1, err, 1);
+            if (need_acc) mbar_wait(acc_empty + 8 * nb, ((ntile >> 1) - 1) & 1, err, 1);
+          }
+          if (k == 8 && MODE == 4) {
+            if (need_slot) slot_ok = mbar_test(slot_bar + 8 * nslot, ((nx / NSL) - 1) & 1);
+            if (need_acc) acc_ok = mbar_test(acc_empty + 8 * nb, ((ntile >> 1) - 1) & 1);
+          }
+          tc_mma_i8_ts(d_t, a_t + k * 8, bd + (uint64_t)(k * BSTEP), IDESC, (first | k) ? 1u : 0u);
+        }
+        tc_commit(a_empty + 8 * slot);
+        if (ACCW && (su & 1) == 1) tc_commit(acc_full + 8 * b);
+        if (MODE == 4) {
+          if (need_slot && !slot_ok) mbar_wait(slot_bar + 8 * nslot, ((nx / NSL) - 1) & 1, err, 1);
+          if (need_acc && !acc_ok) mbar_wait(acc_empty + 8 * nb, ((ntile >> 1) - 1) & 1, err, 1);
+        }
+      }
+    }
+    for (int su = 0; su < (MODE ? 0 : USES); ++su) {
+      const int slot = su % NSL, tile = su >> 1, b = ACC2 ? (tile & 1) : 0;
+      if (ACCW && (su & 1) == 0 && tile >= 2)
+        __all_sync(0xffffffffu, mbar_wait(acc_empty + 8 * b, ((tile >> 1) - 1) & 1, err, 1));
+      if (su >= NSL)
+        __all_sync(0xffffffffu, mbar_wait((HOPW ? a_full : a_empty) + 8 * slot, ((su / NSL) - 1) & 1, err, 1));
+      tc_fence_after();
+      if (leader) {
+        const uint32_t a_t = tmem + 2 * N + (uint32_t)slot * 128;
+        const uint32_t d_t = tmem + b * N;
+        const uint64_t bd = bdesc0 + (uint64_t)(((su * 16) % KST) * BSTEP);
+        const uint32_t first = ACC2 ? (su & 1) : su;  // 0: the tile's first use overwrites
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+          tc_mma_i8_ts(d_t, a_t + k * 8, bd + (uint64_t)(k * BSTEP), IDESC, (first | k) ? 1u : 0u);
+        tc_commit(a_empty + 8 * slot);
+        if (ACCW && (su & 1) == 1) tc_commit(acc_full + 8 * b);
+      }
+      __syncwarp();
+    }
+    if (leader) {
+      tc_commit(fin);
+      mbar_wait(fin, 0, err, 1);
+      const unsigned long long tot = clock64() - t0;
+      s_stop = 1;
+      out[(size_t)blockIdx.x * 4] = tot;
+      out[(size_t)blockIdx.x * 4 + 1] = USES;
+      out[(size_t)blockIdx.x * 4 + 2] = tot;
+    }
+    __syncwarp();
+  } else if (BUSY && ((warp >= 4 && warp < 8) || (warp >= 12 && warp < 16))) {
+    // two warps per sub-partition doing integer work, as the unpack warps
+    // do (BUSY independent shift-and-mask chains per thread), until the
+    // issuer is done; bounded by a count
+    // BUSY 8: FP64 multiply-add chains instead (four per thread), as the
+    // epilogue's statistics
+    uint32_t x[4] = {(uint32_t)tid, (uint32_t)tid * 3u, (uint32_t)tid * 5u, (uint32_t)tid * 7u};
+    double f[4] = {1.0 + tid, 2.0 + tid, 3.0 + tid, 4.0 + tid};
+    for (uint32_t it = 0; it < (1u << 24) && !s_stop; ++it) {
+#pragma unroll
+      for (int r = 0; r < 16; ++r) {
+        if (BUSY == 8) {
+#pragma unroll
+          for (int c = 0; c < 4; ++c) f[c] = fma(f[c], 0.999999, 1e-9);
+        } else {
+#pragma unroll
+          for (int c = 0; c < (BUSY < 4 ? BUSY : 4); ++c) x[c] = ((x[c] * 4u) & 0x80808080u) ^ (x[c] + 0x9e3779b9u);
+        }
+      }
+    }
+    if ((x[0] ^ x[1] ^ x[2] ^ x[3]) == 0x12345678u || f[0] + f[1] + f[2] + f[3] == 1.5) err[3] = 1;  // keeps the work
+  } else if (HOPW && warp >= 8 && warp < 12) {
+    // "unpack" group: waits for each slot's commit, then marks it full (4 arrivals)
+    for (int su = NSL; su < USES; ++su) {
+      const int slot = su % NSL;
+      if (!__all_sync(0xffffffffu, mbar_wait(a_empty + 8 * slot, ((su / NSL) - 1) & 1, err, 1))) break;
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(a_full + 8 * slot);
+    }
+  } else if (ACCW && warp < 4) {
+    // "epilogue" group: takes every tile's accumulator (count 4 on release)
+    for (int tile = 0; tile < USES / 2; ++tile) {
+      const int b = ACC2 ? (tile & 1) : 0;
+      if (!__all_sync(0xffffffffu, mbar_wait(acc_full + 8 * b, (ACC2 ? tile >> 1 : tile) & 1, err, 1))) break;
+      tc_fence_after();
+      uint32_t r[16];
+      tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + b * N, r);
+      tc_wait_ld();
+      if (r[0] == 0x7fffffffu && r[15] == 0x7fffffffu) err[3] = 1;  // keeps the load
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acc_empty + 8 * b);
+    }
+  }
+  if (tid == 0) out[(size_t)blockIdx.x * 4 + 3] = err[2];
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+}
+
+// Two issuers (warps 16, 17) with private rings: issuer j takes the tiles t
+// with t % 2 == j (two uses of MPU MMAs... each tile is 32 MMAs in uses of
+// MPU) into accumulator j, from its own ring of NS2 A slots of MPU * 8
+// columns that its own group of four "unpack" warps frees (warps 8-11 for
+// ring 0, 12-15 for ring 1; each waits for the slot's commit and arrives on
+// its full barrier), and its own "epilogue" group (warps 4j..4j+3) releases
+// its accumulator.  out[0]: the slower issuer's cycles.
+template <int MPU, int NS2>
+__global__ void __launch_bounds__(576, 1) mma_pipe2(unsigned long long* out, unsigned long long* errs) {
+  constexpr int N = 64, KST = 32, USES_T = 32 / MPU;  // uses per tile
+  constexpr int TILES = kIters / 32;
+  static_assert(2 * N + 2 * NS2 * MPU * 8 <= 512, "TMEM columns");
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t* g = smem_raw + (base - raw);
+  // barriers: a_empty[2][NS2], a_full[2][NS2], acc_full[2], acc_empty[2], fin[2]
+  const uint32_t sB = base, a_empty = base + KST * 32 * N, a_full = a_empty + 8 * 2 * NS2,
+                 acc_full = a_full + 8 * 2 * NS2, acc_empty = acc_full + 16, fin = acc_empty + 16;
+  __shared__ uint32_t s_tmem;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < KST * 32 * N / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(g)[i] = 0x01010101u * (i & 3);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&s_tmem))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int t = 0; t < 2 * NS2; ++t) mbar_init(a_empty + 8 * t, 1), mbar_init(a_full + 8 * t, 4);
+    for (int t = 0; t < 2; ++t) mbar_init(acc_full + 8 * t, 1), mbar_init(acc_empty + 8 * t, 4), mbar_init(fin + 8 * t, 1);
+    mbar_fence_init();
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  unsigned long long* err = errs + (size_t)blockIdx.x * 4;
+  if (warp == 16 || warp == 17) {
+    const int j = warp - 16;
+    const bool leader = elect_one();
+    constexpr uint32_t IDESC = idesc_i8(128, N);
+    const uint64_t bdesc0 = sdesc_noswz(sB, N * 16, 128);
+    constexpr uint32_t BSTEP = (2 * N * 16) >> 4;
+    __syncwarp();
+    const unsigned long long t0 = clock64();
+    if (leader) {
+      int u = 0;  // use of this issuer's ring
+      for (int tile = j; tile < TILES; tile += 2) {
+        const int it = tile >> 1;  // this issuer's tile count
+        if (it >= 1) mbar_wait(acc_empty + 8 * j, (it - 1) & 1, err, 1);
+        for (int q = 0; q < USES_T; ++q, ++u) {
+          const int slot = u % NS2;
+          if (u >= NS2) mbar_wait(a_full + 8 * (j * NS2 + slot), ((u / NS2) - 1) & 1, err, 1);
+          tc_fence_after();
+          const uint32_t a_t = tmem + 2 * N + (uint32_t)(j * NS2 + slot) * (MPU * 8);
+          const uint32_t d_t = tmem + j * N;
+          const uint64_t bd = bdesc0 + (uint64_t)(((q * MPU) % KST) * BSTEP);
+#pragma unroll
+          for (int k = 0; k < MPU; ++k)
+            tc_mma_i8_ts(d_t, a_t + k * 8, bd + (uint64_t)(k * BSTEP), IDESC, (q | k) ? 1u : 0u);
+          tc_commit(a_empty + 8 * (j * NS2 + slot));
+        }
+        tc_commit(acc_full + 8 * j);
+      }
+      tc_commit(fin + 8 * j);
+      mbar_wait(fin + 8 * j, 0, err, 1);
+      const unsigned long long tot = clock64() - t0;
+      atomicMax(out + (size_t)blockIdx.x * 4, tot);
+      out[(size_t)blockIdx.x * 4 + 1] = TILES * USES_T;
+      atomicMax(out + (size_t)blockIdx.x * 4 + 2, tot);
+    }
+    __syncwarp();
+  } else if (warp >= 8 && warp < 16) {
+    // ring j's "unpack" group: frees each slot use after its commit
+    const int j = (warp - 8) >> 2;
+    const int uses = (TILES / 2) * USES_T;
+    for (int u = NS2; u < uses; ++u) {
+      const int slot = u % NS2;
+      if (!__all_sync(0xffffffffu, mbar_wait(a_empty + 8 * (j * NS2 + slot), ((u / NS2) - 1) & 1, err, 1))) break;
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(a_full + 8 * (j * NS2 + slot));
+    }
+  } else if (warp < 8) {
+    // accumulator j's "epilogue" group
+    const int j = warp >> 2;
+    for (int it = 0; it < TILES / 2; ++it) {
+      if (!__all_sync(0xffffffffu, mbar_wait(acc_full + 8 * j, it & 1, err, 1))) break;
+      tc_fence_after();
+      uint32_t r[16];
+      tc_ld16(tmem + ((uint32_t)((warp & 3) * 32) << 16) + j * N, r);
+      tc_wait_ld();
+      if (r[0] == 0x7fffffffu && r[15] == 0x7fffffffu) err[3] = 1;  // keeps the load
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acc_empty + 8 * j);
+    }
   }
   if (tid == 0) out[(size_t)blockIdx.x * 4 + 3] = err[2];
   tc_fence_before();
@@ -563,6 +1019,35 @@ int run_kind(int kind, int issuers, int sms, Result& r) {
     case 31: return N > 64 ? 1 : launch_and_read(mma_ring<N, 3, 16, 0, 0>, sms, 256, 150 * 1024, 1, 0, r);
     case 32: return N > 64 ? 1 : launch_and_read(mma_ring<N, 1, 16, 0, 0>, sms, 256, 150 * 1024, 1, 0, r);
     case 33: return N > 64 ? 1 : launch_and_read(mma_ring<N, 3, 16, 2>, sms, 256, 150 * 1024, 1, 0, r);
+    case 34: return N > 64 ? 1 : launch_and_read(mma_ring<N, 3, 16, 0, 1, 1>, sms, 256, 150 * 1024, 1, 0, r);
+    case 35: return N > 64 ? 1 : launch_and_read(mma_ring<N, 2, 16, 0, 1, 1>, sms, 256, 150 * 1024, 1, 0, r);
+    case 36: return N > 64 ? 1 : launch_and_read(mma_ring<N, 6, 8, 0, 1, 1>, sms, 256, 150 * 1024, 1, 0, r);
+    case 37: return N > 64 ? 1 : launch_and_read(mma_ring<N, 3, 16, 0, 1, 0, 1>, sms, 256, 150 * 1024, 1, 0, r);
+    case 38: return N > 64 ? 1 : launch_and_read(mma_ring<N, 3, 16, 0, 1, 0, 2>, sms, 256, 150 * 1024, 1, 0, r);
+    case 39: return N > 64 ? 1 : launch_and_read(mma_ring<N, 3, 16, 0, 1, 0, 3>, sms, 256, 150 * 1024, 1, 0, r);
+    case 40: return N != 64 ? 1 : launch_and_read(mma_pipe<0, 0, 0>, sms, 576, 150 * 1024, 1, 0, r);
+    case 41: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 0, 0>, sms, 576, 150 * 1024, 1, 0, r);
+    case 42: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 1, 0>, sms, 576, 150 * 1024, 1, 0, r);
+    case 43: return N != 64 ? 1 : launch_and_read(mma_pipe<0, 0, 1>, sms, 576, 150 * 1024, 1, 0, r);
+    case 44: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 1, 1>, sms, 576, 150 * 1024, 1, 0, r);
+    case 45: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 1, 1, 1>, sms, 576, 150 * 1024, 1, 0, r);
+    case 46: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 1, 1, 2>, sms, 576, 150 * 1024, 1, 0, r);
+    case 47: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 1, 1, 3>, sms, 576, 150 * 1024, 1, 0, r);
+    case 48: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 1, 1, 4>, sms, 576, 150 * 1024, 1, 0, r);
+    case 49: return N != 64 ? 1 : launch_and_read(mma_pipe<0, 0, 1, 1>, sms, 576, 150 * 1024, 1, 0, r);
+    case 50: return N != 64 ? 1 : launch_and_read(mma_pipe<0, 0, 1, 3>, sms, 576, 150 * 1024, 1, 0, r);
+    case 51: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 1, 1, 0, 2>, sms, 576, 150 * 1024, 1, 0, r);
+    case 52: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 1, 1, 3, 2>, sms, 576, 150 * 1024, 1, 0, r);
+    case 53: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 1, 1, 0, 4>, sms, 576, 150 * 1024, 1, 0, r);
+    case 54: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 1, 1, 3, 4>, sms, 576, 150 * 1024, 1, 0, r);
+    case 55: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 1, 1, 1, 0, 1>, sms, 576, 150 * 1024, 1, 0, r);
+    case 56: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 1, 1, 1, 2, 1>, sms, 576, 150 * 1024, 1, 0, r);
+    case 57: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 1, 1, 1, 4, 1>, sms, 576, 150 * 1024, 1, 0, r);
+    case 58: return N != 64 ? 1 : launch_and_read(mma_pipe2<8, 3>, sms, 576, 150 * 1024, 1, 0, r);
+    case 59: return N != 64 ? 1 : launch_and_read(mma_pipe2<8, 2>, sms, 576, 150 * 1024, 1, 0, r);
+    case 60: return N != 64 ? 1 : launch_and_read(mma_pipe2<16, 1>, sms, 576, 150 * 1024, 1, 0, r);
+    case 61: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 1, 1, 1, 8, 1>, sms, 576, 150 * 1024, 1, 0, r);
+    case 62: return N != 64 ? 1 : launch_and_read(mma_pipe<1, 1, 1, 0, 8>, sms, 576, 150 * 1024, 1, 0, r);
     default: return 1;
   }
 }
@@ -593,5 +1078,38 @@ extern "C" int kg_bench_mma_rate(int kind, int n_cols, int issuers, double* cycl
   if (cycles_per_mma) *cycles_per_mma = r.cycles_per_mma;
   if (side_cycles_per_op) *side_cycles_per_op = r.side_cycles_per_op;
   if (err) *err = r.err;
+  return rc;
+}
+
+// Timeline of CTA 0 on a ring of nsl (1..3) A slots of 16 MMAs (N = 64) in
+// MMA form `form` (see mma_form), or (nsl 4) one slot of 48 MMAs, one CTA per
+// SM: 3 clocks per use (wait began, wait returned, use issued), relative to
+// the first use; out holds 3 * 256 values.  0 on success.
+extern "C" int kg_bench_mma_timeline(int nsl, int form, unsigned long long* out) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t n = 3 * (kIters / 16);
+  unsigned long long *d = nullptr, *e = nullptr;
+  if (cudaMalloc(&d, n * 8) != cudaSuccess) return 3;
+  if (cudaMalloc(&e, (size_t)sms * 4 * 8) != cudaSuccess) {
+    cudaFree(d);
+    return 3;
+  }
+  cudaMemset(e, 0, (size_t)sms * 4 * 8);
+  // nsl 1..3 with form 0..2; nsl 4: one slot of 48 MMAs per use (form 0)
+  auto k = nsl == 4 ? mma_ring_timeline<1, 0, 48>
+           : form == 1 ? (nsl == 1 ? mma_ring_timeline<1, 1> : nsl == 2 ? mma_ring_timeline<2, 1> : mma_ring_timeline<3, 1>)
+           : form == 2 ? (nsl == 1 ? mma_ring_timeline<1, 2> : nsl == 2 ? mma_ring_timeline<2, 2> : mma_ring_timeline<3, 2>)
+                       : (nsl == 1 ? mma_ring_timeline<1> : nsl == 2 ? mma_ring_timeline<2> : mma_ring_timeline<3>);
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+  int rc = 0;
+  for (int rep = 0; rep < 2 && rc == 0; ++rep) {
+    k<<<sms, 128, 100 * 1024>>>(d, e);
+    if (cudaDeviceSynchronize() != cudaSuccess) rc = 2;
+  }
+  if (rc == 0 && cudaMemcpy(out, d, n * 8, cudaMemcpyDeviceToHost) != cudaSuccess) rc = 2;
+  cudaFree(d);
+  cudaFree(e);
   return rc;
 }
