@@ -829,13 +829,22 @@ def files_cols_leg(Xh, n, U, y, keep, local, seed=51):
             dt = time.perf_counter() - t0
             if r.returncode != 0:
                 raise RuntimeError(f"{tag}: {r.stderr[-500:]}")
-            return open(out + ".count").read(), dt
+            return open(out + ".count").read(), dt, r.stderr
 
         run("warm", False)
-        c_ours, s_ours = run("ours", False)
-        c_ref, s_ref = run("ref", True) if reference_binary() else (None, None)
+        c_ours, s_ours, err_ours = run("ours", False)
+        c_ref, s_ref, _ = run("ref", True) if reference_binary() else (None, None, None)
     tested = int(c_ours.split("\t")[1])
-    return {"kmers": m, "ours_seconds": s_ours, "ours_tests_per_s": tested / s_ours,
+    # the program's own milestones ("[TIME] <what> <seconds> s", from its start)
+    marks = {}
+    for line in (err_ours or "").splitlines():
+        if line.startswith("[TIME] ") and line.endswith(" s"):
+            what, _, sec = line[7:-2].rpartition(" ")
+            try:
+                marks[what] = float(sec)
+            except ValueError:
+                pass
+    return {"kmers": m, "ours_seconds": s_ours, "ours_tests_per_s": tested / s_ours, "ours_milestones_s": marks,
             "reference_seconds": s_ref, "reference_tests_per_s": tested / s_ref if s_ref else None,
             "speedup": s_ref / s_ours if s_ref else None, "count_lines_identical": c_ours == c_ref,
             "write_seconds": t_w, "threads": threads,

@@ -134,6 +134,15 @@ int kg_fetch(kg_ctx* ctx, kg_result* res, kg_stats* stats);
 int kg_launch_device_stats(kg_ctx* ctx, const uint64_t* d_xbits, uint64_t n_kmers,
                            uint32_t words_per_kmer, void* stream);
 
+/* Allocates now the buffers that kg_run_host needs for a batch of n_kmers
+ * pageable rows of words_per_kmer words (its device chunks and page-locked
+ * staging buffers, 2 x min(512 MB, the batch) of each), so that a program
+ * can pay for them while it still reads its inputs, e.g. on the thread that
+ * created the context.  They are kept for later calls; kg_run_host grows
+ * them when a batch needs more.  Replaces nothing in the reference (it has
+ * no device buffers). */
+int kg_reserve_host(kg_ctx* ctx, uint64_t n_kmers, uint32_t words_per_kmer);
+
 /* Page-locked host memory for packed rows, so that kg_run_host copies at full
  * link speed without staging; NULL on failure.  Free with kg_host_free. */
 void* kg_host_alloc(size_t bytes);

@@ -127,6 +127,7 @@ def lib():
     L.kg_probe_h2d_gbs.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     L.kg_multi_shape.argtypes = [vp, ctypes.POINTER(_TileShape)]
     L.kg_set_wait_limit.argtypes = [vp, ctypes.c_uint64]
+    L.kg_reserve_host.argtypes = [vp, ctypes.c_uint64, ctypes.c_uint32]
     L.kg_inject_stall.argtypes = [vp, ctypes.c_uint64]
     L.kg_version.restype = ctypes.c_char_p
     L.kg_host_alloc.argtypes = [ctypes.c_size_t]
@@ -356,6 +357,10 @@ class Kgwas:
 
     def last_kernel(self) -> str:
         return self._L.kg_last_kernel(self._h).decode()
+
+    def reserve_host(self, n_kmers: int, words_per_kmer: int):
+        """Allocate now the buffers run_host needs for a batch of this shape (kg_reserve_host)."""
+        self._check(self._L.kg_reserve_host(self._h, int(n_kmers), int(words_per_kmer)), "kg_reserve_host")
 
     def set_wait_limit(self, wait_ns: int):
         """Limit of every pipeline wait on the device, in ns (0: the default 2 s)."""

@@ -556,14 +556,19 @@ bool want_stats(const kg_stats* st) {
 // `runs`, each chunk is scanned for runs of equal rows while it is staged and
 // only the first row of each run is copied and tested, weighted by its run's
 // length (ctx->run_first / run_len / unique_rows describe the runs).
-int run_host_once(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t wpk, bool stats, bool runs) {
+// Rows per chunk of the host pipeline for m rows of wpk words: 512 MB of
+// rows (KG_CHUNK_MB), at most m.
+uint64_t host_chunk_rows(uint64_t m, uint32_t wpk) {
   const size_t row = (size_t)wpk * 8;
   size_t want = (size_t)512 << 20;
   if (const char* v = std::getenv("KG_CHUNK_MB")) want = (size_t)std::max(1, std::atoi(v)) << 20;
   uint64_t per = std::max<uint64_t>(1, want / row);
-  if (per > m) per = m;
-  const size_t bytes = (size_t)per * row;
-  const bool pinned = !runs && is_pinned(xbits);
+  return per > m ? m : per;
+}
+
+// The device chunks (and, with `staging`, the pinned staging buffers) of the
+// host pipeline, at least `bytes` each; kept for later calls.
+int ensure_chunks(kg_ctx* ctx, size_t bytes, bool staging) {
   if (ctx->chunk_bytes < bytes) {
     for (int b = 0; b < NBUF; ++b) {
       dfree(ctx->dChunk[b]);
@@ -574,9 +579,18 @@ int run_host_once(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t wpk, 
     for (int b = 0; b < NBUF; ++b) KG_CUDA(cudaMalloc((void**)&ctx->dChunk[b], bytes), "cudaMalloc(chunk)");
     ctx->chunk_bytes = bytes;
   }
-  if (!pinned)
+  if (staging)
     for (int b = 0; b < NBUF; ++b)
       if (!ctx->hStage[b]) KG_CUDA(cudaHostAlloc(&ctx->hStage[b], ctx->chunk_bytes, cudaHostAllocDefault), "cudaHostAlloc");
+  return KG_OK;
+}
+
+int run_host_once(kg_ctx* ctx, const uint64_t* xbits, uint64_t m, uint32_t wpk, bool stats, bool runs) {
+  const size_t row = (size_t)wpk * 8;
+  const uint64_t per = host_chunk_rows(m, wpk);
+  const size_t bytes = (size_t)per * row;
+  const bool pinned = !runs && is_pinned(xbits);
+  if (int rc = ensure_chunks(ctx, bytes, !pinned)) return rc;
   if (runs) {
     ctx->run_first.clear();
     ctx->run_len.clear();
@@ -728,6 +742,13 @@ extern "C" int kg_launch_device_stats(kg_ctx* ctx, const uint64_t* d_x, uint64_t
   rc = kg_launch_device(ctx, d_x, m, wpk, stream);
   if (rc) ctx->pend_stats = false;
   return rc;
+}
+
+extern "C" int kg_reserve_host(kg_ctx* ctx, uint64_t m, uint32_t wpk) {
+  if (!ctx) return KG_ERR_INVALID;
+  if (m == 0 || wpk == 0) return ctx->fail(KG_ERR_INVALID, "kg_reserve_host: empty batch");
+  KG_CUDA(cudaSetDevice(ctx->opts.device), "cudaSetDevice");
+  return ensure_chunks(ctx, (size_t)host_chunk_rows(m, wpk) * wpk * 8, true);
 }
 
 extern "C" void* kg_host_alloc(size_t bytes) {

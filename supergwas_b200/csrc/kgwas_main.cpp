@@ -163,6 +163,15 @@ struct Gpu {
     o.log10_thresh = cfg.log10_thresh;
     th = std::thread([this, o] { rc = kg_create(&ctx, &o); });
   }
+  // Once the batch's shape is known: the host pipeline's buffers, allocated
+  // on the same thread after the context (while the inputs are still read).
+  void reserve(uint64_t n_kmers, uint32_t words_per_kmer) {
+    std::thread prev = std::move(th);
+    th = std::thread([this, n_kmers, words_per_kmer, p = std::move(prev)]() mutable {
+      if (p.joinable()) p.join();
+      if (rc == KG_OK && ctx) kg_reserve_host(ctx, n_kmers, words_per_kmer);  // kg_run_host retries on failure
+    });
+  }
   void open(const Config& cfg) {
     if (!th.joinable() && !ctx) start(cfg);
     if (th.joinable()) th.join();
@@ -382,6 +391,7 @@ static void run_cols(const Config& cfg) {  // src/kgwas.cpp:168-307
   vector<string> kmers;
   std::thread kt([&] { kmers = kgio::load_kmers(kmers_gz, N); });
   const uint32_t W = kgio::words_per_kmer(n);
+  if (N > 0) g.reserve(N, W);
   HostWords X;
   X.alloc((size_t)N * W);
   const char* kb = std::getenv("KGWAS_KBITS");
