@@ -499,6 +499,7 @@ static void run_rows(const Config& cfg) {  // src/kgwas.cpp:343-522
   uint64_t passed = 0;
   size_t BATCH = (size_t)1 << 22;
   if (const char* v = std::getenv("KGWAS_ROWS_BATCH")) BATCH = (size_t)std::max(1L, std::atol(v));
+  g.reserve(BATCH, W);  // while the first batch is read
   struct Batch {
     vector<string> kmers;
     vector<uint64_t> packed;
