@@ -16,8 +16,9 @@
  * Conventions
  *   - Every function returns KG_OK (0) or a KG_ERR_* code and never exits
  *     the process; kg_last_error() describes the last failure of a context.
- *   - One context per GPU and per host thread.  A context owns its device
- *     buffers and its CUDA stream.
+ *   - One context per GPU.  A context owns its device buffers and its CUDA
+ *     stream; calls on it must not overlap, and it may pass from one host
+ *     thread to another between calls (every call selects its GPU).
  *   - Packed k-mer rows: k-mer-major, `words_per_kmer` uint64 words per
  *     k-mer (even, so every row starts on a 16-byte boundary); overlap
  *     sample i is bit (i % 64) of word (i / 64); bits at i >= n are ignored.

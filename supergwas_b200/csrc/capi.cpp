@@ -736,6 +736,7 @@ int kg_launch_device(kg_ctx* ctx, const uint64_t* d_x, uint64_t m, uint32_t wpk,
 // internal entry (used by kg_fetch's caller through kg_launch_device_stats).
 extern "C" int kg_launch_device_stats(kg_ctx* ctx, const uint64_t* d_x, uint64_t m, uint32_t wpk, void* stream) {
   if (!ctx) return KG_ERR_INVALID;
+  KG_CUDA(cudaSetDevice(ctx->opts.device), "cudaSetDevice");  // the statistics buffers live on the context's GPU
   int rc = ensure_stats(ctx, m);
   if (rc) return rc;
   ctx->pend_stats = true;
@@ -753,7 +754,8 @@ extern "C" int kg_reserve_host(kg_ctx* ctx, uint64_t m, uint32_t wpk) {
 
 extern "C" void* kg_host_alloc(size_t bytes) {
   void* p = nullptr;
-  if (cudaHostAlloc(&p, bytes ? bytes : 1, cudaHostAllocDefault) != cudaSuccess) {
+  // portable: page-locked for every GPU's context, whichever device is current
+  if (cudaHostAlloc(&p, bytes ? bytes : 1, cudaHostAllocPortable) != cudaSuccess) {
     cudaGetLastError();
     return nullptr;
   }
